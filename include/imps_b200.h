@@ -1,0 +1,242 @@
+/*
+ * imps_b200 -- C ABI of the B200 implementation of the InfiniteMPSAlgorithms
+ * VUMPS / IDMRG / TDVP inner loop (guochu/InfiniteMPSAlgorithms).
+ *
+ * Every entry point takes plain pointers and sizes.  Tensors are column-major
+ * ComplexF64 arrays (interleaved re, im doubles), i.e. exactly the memory of a
+ * Julia `Array{ComplexF64}` of the reference, so a Julia `ccall` passes
+ * `pointer(A)` directly.  Device memory is owned by the library behind the
+ * opaque handles below; `*_dev` entry points take device pointers instead.
+ *
+ * Index conventions (reference src/algorithms/groundstates/effective.jl:3-5):
+ *   site tensors A[a, s, b]       shape (Dl, d, Dr)
+ *   left envs    GL[bra, w, ket]  shape (Dl, m, Dl)
+ *   right envs   GR[ket, w, bra]  shape (Dr, n, Dr)
+ *   MPO tensors  W[wl, u, wr, s]  shape (m, d, n, d), u = output (bra) leg
+ *
+ * Return value: an IMPS_* status.  IMPS_NOT_CONVERGED is a warning (the
+ * reference only emits `@warn`), the result is still written.
+ *
+ * Threading: a context owns one CUDA stream; calls on one context must be
+ * serialised by the caller (one context per host thread).
+ */
+#ifndef IMPS_B200_H
+#define IMPS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  IMPS_OK = 0,
+  IMPS_NOT_CONVERGED = 1,   /* warning: iteration limit reached, result written   */
+  IMPS_DIM_MISMATCH = -1,   /* reference: DimensionMismatch                        */
+  IMPS_INVALID_ARG = -2,    /* reference: ArgumentError                            */
+  IMPS_OOM = -3,            /* device allocation failed                            */
+  IMPS_CUDA_ERROR = -4,     /* CUDA / cuSOLVER failure                             */
+  IMPS_TIMEOUT = -5,        /* a bounded device wait gave up                       */
+  IMPS_NO_DEVICE = -6       /* no CUDA device visible                              */
+};
+
+/* Precision modes of the Heff / transfer contractions. */
+enum {
+  IMPS_PREC_FP64 = 0,       /* plain method: FP64 end to end                       */
+  IMPS_PREC_SPLIT_I8 = 1    /* int8 split products on tcgen05, exact int32 sums    */
+};
+
+/* Field selectors for imps_state_get / imps_state_set. */
+enum { IMPS_AL = 0, IMPS_AR = 1, IMPS_C = 2, IMPS_AC = 3 };
+
+typedef struct imps_ctx imps_ctx;
+typedef struct imps_mpo imps_mpo;
+typedef struct imps_state imps_state;
+typedef struct imps_envs imps_envs;
+
+/* KrylovKit `ConvergenceInfo` equivalent (converged, numiter, numops, normres). */
+typedef struct {
+  int32_t converged;
+  int32_t numiter;
+  int32_t numops;
+  int32_t pad;
+  double normres;
+  double value_re;   /* eigenvalue (eigsolve) */
+  double value_im;
+} imps_krylov_info;
+
+/* Per-build statistics of the environment solver. */
+typedef struct {
+  int32_t solves;
+  int32_t gmres_iters;
+  int32_t gmres_ops;
+  int32_t pushes;
+  int32_t converged;   /* 1 when every linsolve met its tolerance */
+  int32_t pad;
+  double max_normres;
+} imps_env_info;
+
+/* Gauge-fixing iteration summary (uniform_leftorth!/uniform_rightorth!). */
+typedef struct {
+  int32_t niter;
+  int32_t converged;
+  double err;
+} imps_gauge_info;
+
+/* One VUMPS iteration summary. */
+typedef struct {
+  double galerkin;            /* calc_galerkin after the iteration              */
+  double energy_re;           /* expectationvalue(psi, H, envs)                 */
+  double energy_im;
+  int32_t ac_matvecs;         /* AC Heff applications in the eigensolves        */
+  int32_t c_matvecs;
+  int32_t gauge_iters;
+  int32_t env_gmres_ops;
+  imps_env_info env;
+} imps_vumps_info;
+
+/* ---------------------------------------------------------------- context */
+/* Replaces: the implicit Julia process state (no reference counterpart). */
+int imps_ctx_create(int device, imps_ctx** out);
+int imps_ctx_destroy(imps_ctx* ctx);
+/* Use a caller-owned cudaStream_t (e.g. the host framework's current stream). */
+int imps_ctx_set_stream(imps_ctx* ctx, void* cuda_stream);
+/* Precision of the Heff/transfer contractions: IMPS_PREC_FP64 or
+ * IMPS_PREC_SPLIT_I8 with `nslices` int8 slices per operand (2..7); nslices <= 0
+ * selects slices per call from the requested solver tolerance. */
+int imps_ctx_set_precision(imps_ctx* ctx, int mode, int nslices);
+int imps_ctx_synchronize(imps_ctx* ctx);
+const char* imps_ctx_last_error(const imps_ctx* ctx);
+const char* imps_status_string(int status);
+/* Kernel timing with CUDA events on the context stream, per kernel class. */
+int imps_ctx_profile(imps_ctx* ctx, int enable);
+int imps_ctx_profile_get(imps_ctx* ctx, const char* kernel_class, int64_t* launches, double* total_ms,
+                         double* work);
+int imps_ctx_profile_reset(imps_ctx* ctx);
+/* counters[0..4] = AC applies, C applies, pushes, GEMM launches, all kernel launches */
+int imps_ctx_counters(imps_ctx* ctx, int64_t* counters);
+
+/* -------------------------------------------------------------------- MPO */
+/* Replaces SparseIMPO / SchurMPOTensor storage (src/operators/mpohamiltonian.jl:33-52):
+ * W[l] is the dense tompotensor(H[l]) of shape (m[l], d[l], n[l], d[l])
+ * (src/algorithms/groundstates/envs.jl:332). */
+int imps_mpo_create(imps_ctx* ctx, int N, const int* m, const int* d, const int* n, const double* const* W,
+                    imps_mpo** out);
+int imps_mpo_destroy(imps_mpo* mpo);
+
+/* ------------------------------------------------------------------ state */
+/* Replaces CanonicalIMPS (src/states/canonicalmps.jl:17-40).  chi[l] is the
+ * bond dimension right of site l (bond N-1 == bond 0), d[l] the physical dim. */
+int imps_state_create(imps_ctx* ctx, int N, const int* d, const int* chi, imps_state** out);
+int imps_state_destroy(imps_state* st);
+int imps_state_set(imps_state* st, int field, int site, const double* host);
+int imps_state_get(const imps_state* st, int field, int site, double* host);
+int imps_state_copy(imps_state* dst, const imps_state* src);
+/* CanonicalIMPS(As): gaugefix!(:LR) from C0 = I, AC = AL*C
+ * (src/states/canonicalmps.jl:151-170). */
+int imps_state_canonicalize(imps_state* st, const double* const* As, double tol, int maxiter,
+                            imps_gauge_info* info);
+/* CanonicalIMPS(ALs, C0): gaugefix!(:R), AC = AL*C (src/states/canonicalmps.jl:180-195). */
+int imps_state_from_al(imps_state* st, const double* const* ALs, const double* C0, double tol, int maxiter,
+                       imps_gauge_info* info);
+/* gauge_step! (src/algorithms/groundstates/vumps.jl:257-266): keep st->AL, right gauge
+ * fix from C0 = st->C[N] for AR and C, then AC = AL*C. */
+int imps_gauge_step(imps_state* st, double tol, int maxiter, imps_gauge_info* info);
+/* dot(psi, psi) (src/states/canonicalmps.jl:262-269). */
+int imps_state_dot(imps_state* st, double* re, double* im);
+
+/* ------------------------------------------------------------ environments */
+/* Replaces DMRGCache(psi, ::SparseIMPO) (src/algorithms/groundstates/envs.jl:248-257, 321-518). */
+int imps_envs_create(imps_ctx* ctx, const imps_state* st, const imps_mpo* mpo, imps_envs** out);
+int imps_envs_destroy(imps_envs* envs);
+/* DMRGCache constructor / recalculate! (envs.jl:321-546); warm != 0 uses the
+ * current contents as init_lefts / init_rights. */
+int imps_envs_build(imps_envs* envs, const imps_state* st, const imps_mpo* mpo, double tol, int maxiter,
+                    int krylovdim, int warm, imps_env_info* info);
+/* side 0: lefts[site], side 1: rights[site] */
+int imps_envs_get(const imps_envs* envs, int side, int site, double* host);
+int imps_envs_set(imps_envs* envs, int side, int site, const double* host);
+
+/* ------------------------------------------------- effective Hamiltonians */
+/* MPO_AC_Hamiltonian action (src/algorithms/groundstates/effective.jl:66-68, 90-102). */
+int imps_ac_apply(imps_envs* envs, const imps_mpo* mpo, int site, const double* x, double* y);
+int imps_ac_apply_dev(imps_envs* envs, const imps_mpo* mpo, int site, const void* x_dev, void* y_dev);
+/* MPO_C_Hamiltonian action (effective.jl:52-54, 72-76): GL = lefts[site+1], GR = rights[site]. */
+int imps_c_apply(imps_envs* envs, int site, const double* x, double* y);
+int imps_c_apply_dev(imps_envs* envs, int site, const void* x_dev, void* y_dev);
+
+/* --------------------------------------------------------- transfer pushes */
+/* push_env_left(L, above, below) / push_env_right(R, above, below)
+ * (src/transfermatrix.jl:5-7, 23-26, 54-66); above, below: (Dl, d, Dr). */
+int imps_push_left(imps_ctx* ctx, int Dl, int d, int Dr, const double* L, const double* above,
+                   const double* below, double* out);
+int imps_push_right(imps_ctx* ctx, int Dl, int d, int Dr, const double* R, const double* above,
+                    const double* below, double* out);
+/* Schur MPO pushes (envs.jl:199-231, transfer_leftenv!/transfer_rightenv! :591-604)
+ * with the MPO tensor of site `site`. */
+int imps_push_mpo_left(imps_ctx* ctx, const imps_mpo* mpo, int site, int Dl, int Dr, const double* L,
+                       const double* A, double* out);
+int imps_push_mpo_right(imps_ctx* ctx, const imps_mpo* mpo, int site, int Dl, int Dr, const double* R,
+                        const double* A, double* out);
+
+/* --------------------------------------------------------- factorizations */
+/* leftorth(M; alg = QRpos()) / rightorth(M; alg = LQpos()) (FiniteMPSAlgorithms,
+ * used at src/states/ortho.jl:150, 188, 214-225).  M is m x n column-major. */
+int imps_qrpos(imps_ctx* ctx, int m, int n, const double* M, double* Q, double* R);
+int imps_lqpos(imps_ctx* ctx, int m, int n, const double* M, double* L, double* Q);
+/* regauge!(AC, C) (src/states/ortho.jl:214-219): AL = Q(AC) Q(C)^H. */
+int imps_regauge(imps_ctx* ctx, int Dl, int d, int Dr, const double* AC, const double* C, double* AL);
+
+/* ----------------------------------------------------------- Krylov solvers */
+/* fixedpoint(H_AC, x0, :SR, Lanczos) (src/utility.jl:180-186, 379-393). */
+int imps_eigsolve_ac(imps_envs* envs, const imps_mpo* mpo, int site, const double* x0, double* x, double tol,
+                     int krylovdim, int maxiter, int eager, imps_krylov_info* info);
+int imps_eigsolve_c(imps_envs* envs, int site, const double* x0, double* x, double tol, int krylovdim,
+                    int maxiter, int eager, imps_krylov_info* info);
+/* integrate(H, x, dt, Lanczos) -> exponentiate (src/algorithms/timeevo/tdvp.jl:14-20). */
+int imps_exponentiate_ac(imps_envs* envs, const imps_mpo* mpo, int site, double dt_re, double dt_im,
+                         const double* x0, double* x, double tol, int krylovdim, int maxiter,
+                         imps_krylov_info* info);
+int imps_exponentiate_c(imps_envs* envs, int site, double dt_re, double dt_im, const double* x0, double* x,
+                        double tol, int krylovdim, int maxiter, imps_krylov_info* info);
+/* linsolve / integrate on a diagonal operator diag(dvals) of length n (the
+ * reference's solver-level known-answer tests, test/algorithms/api.jl:248-251, 469-478). */
+int imps_linsolve_diag(imps_ctx* ctx, int64_t n, const double* dvals, const double* b, const double* x0,
+                       double a0, double a1, double tol, int krylovdim, int maxiter, double* x,
+                       imps_krylov_info* info);
+int imps_exponentiate_diag(imps_ctx* ctx, int64_t n, const double* dvals, double dt_re, double dt_im,
+                           const double* x0, double* x, double tol, int krylovdim, int maxiter,
+                           imps_krylov_info* info);
+
+/* ------------------------------------------------------------- observables */
+/* calc_galerkin (src/algorithms/groundstates/vumps.jl:111-124). */
+int imps_galerkin(imps_envs* envs, const imps_mpo* mpo, const imps_state* st, double* eps);
+/* expectationvalue(psi, H::SparseIMPO, envs) (src/observables/expval.jl:93-112). */
+int imps_energy(imps_envs* envs, const imps_mpo* mpo, imps_state* st, double* re, double* im);
+/* expectationvalue(psi, (site,) => O) (src/observables/expval.jl:33-37); O is d x d. */
+int imps_local_expval(imps_state* st, int site, const double* O, double* re, double* im);
+
+/* -------------------------------------------------------------- algorithms */
+/* localupdate_step! (vumps.jl:241-253): per site AC and C eigensolves + regauge!,
+ * candidate ALs written into st->AL. */
+int imps_vumps_localupdate(imps_envs* envs, const imps_mpo* mpo, imps_state* st, double tol, int krylovdim,
+                           int maxiter, int eager, int32_t* ac_matvecs, int32_t* c_matvecs);
+/* One full VUMPS iteration (vumps.jl:296-318) for the outer-loop index `iter`
+ * (1-based) and the previous Galerkin error `eps`, with the reference's dynamic
+ * tolerances (Defaults, src/utility.jl:308-320). */
+int imps_vumps_iter(imps_envs* envs, const imps_mpo* mpo, imps_state* st, int iter, double eps,
+                    imps_vumps_info* info);
+/* timestep(psi, H, dt, TDVP(), envs) (src/algorithms/timeevo/tdvp.jl:34-53). */
+int imps_tdvp_step(imps_envs* envs, const imps_mpo* mpo, imps_state* st, double dt_re, double dt_im,
+                   double tol, int krylovdim, int maxiter, double gauge_tol, int gauge_maxiter,
+                   imps_krylov_info* info);
+/* _localupdate_sweep_idmrg! (src/algorithms/groundstates/idmrg.jl:12-33); returns the
+ * last eigenvalue in *E and ||C[0] - C_old|| in *eps. */
+int imps_idmrg_sweep(imps_envs* envs, const imps_mpo* mpo, imps_state* st, double tol, int krylovdim,
+                     int maxiter, int eager, double* E, double* eps);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* IMPS_B200_H */

@@ -1,0 +1,25 @@
+// Observables and algorithm steps (see algos.cu).
+#pragma once
+#include "imps_internal.h"
+#include "krylov.h"
+
+namespace imps {
+double galerkin(Context* ctx, imps_envs* E, const imps_mpo* H, const imps_state* st);
+cplx energy(Context* ctx, imps_envs* E, const imps_mpo* H, imps_state* st);
+cplx local_expval(Context* ctx, imps_state* st, int site, const cplx* O);
+KrylovResult eigsolve_ac(Context* ctx, imps_envs* E, const imps_mpo* H, int site, const dcplx* x0, dcplx* x,
+                         double tol, int kdim, int maxiter, bool eager);
+KrylovResult eigsolve_c(Context* ctx, imps_envs* E, int site, const dcplx* x0, dcplx* x, double tol, int kdim,
+                        int maxiter, bool eager);
+KrylovResult expo_ac(Context* ctx, imps_envs* E, const imps_mpo* H, int site, cplx dt, const dcplx* x0, dcplx* x,
+                     double tol, int kdim, int maxiter);
+KrylovResult expo_c(Context* ctx, imps_envs* E, int site, cplx dt, const dcplx* x0, dcplx* x, double tol, int kdim,
+                    int maxiter);
+void vumps_localupdate(Context* ctx, imps_envs* E, const imps_mpo* H, imps_state* st, double tol, int kdim, int maxiter,
+                       bool eager, int* nac, int* nc);
+imps_vumps_info vumps_iter(Context* ctx, imps_envs* E, const imps_mpo* H, imps_state* st, int iter, double eps);
+KrylovResult tdvp_step(Context* ctx, imps_envs* E, const imps_mpo* H, imps_state* st, cplx dt, double tol, int kdim,
+                       int maxiter, double gauge_tol, int gauge_maxiter);
+void idmrg_sweep(Context* ctx, imps_envs* E, const imps_mpo* H, imps_state* st, double tol, int kdim, int maxiter,
+                 bool eager, double* Eout, double* epsout);
+}  // namespace imps

@@ -1,0 +1,282 @@
+// Internal declarations of the imps_b200 runtime (not part of the C ABI).
+//
+// Storage convention everywhere: column-major complex128 (interleaved re, im),
+// exactly the Julia layout of the reference, so a host array of the reference
+// can be copied byte for byte.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cusolverDn.h>
+
+#include <complex>
+#include <cstdint>
+#include <cstdio>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/imps_b200.h"
+
+namespace imps {
+
+using cplx = std::complex<double>;
+using dcplx = double2;  // device complex
+
+// Error carried from the depths of the runtime to the C ABI.
+struct Error : public std::runtime_error {
+  int status;
+  Error(int s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+#define IMPS_CUDA(call)                                                               \
+  do {                                                                                \
+    cudaError_t e_ = (call);                                                          \
+    if (e_ != cudaSuccess) {                                                          \
+      if (e_ == cudaErrorMemoryAllocation)                                            \
+        throw ::imps::Error(IMPS_OOM, std::string("out of device memory: ") + #call); \
+      throw ::imps::Error(IMPS_CUDA_ERROR, std::string(cudaGetErrorString(e_)) +      \
+                                               " at " + __FILE__ + ":" +              \
+                                               std::to_string(__LINE__));             \
+    }                                                                                 \
+  } while (0)
+
+#define IMPS_SOLVER(call)                                                                 \
+  do {                                                                                    \
+    cusolverStatus_t s_ = (call);                                                         \
+    if (s_ != CUSOLVER_STATUS_SUCCESS)                                                    \
+      throw ::imps::Error(IMPS_CUDA_ERROR, std::string("cusolver status ") +             \
+                                               std::to_string((int)s_) + " at " +         \
+                                               __FILE__ + ":" + std::to_string(__LINE__)); \
+  } while (0)
+
+#define IMPS_REQUIRE(cond, status, msg)        \
+  do {                                         \
+    if (!(cond)) throw ::imps::Error(status, msg); \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// Device buffers
+// ---------------------------------------------------------------------------
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  explicit DevBuf(size_t b) { alloc(b); }
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : ptr(o.ptr), bytes(o.bytes) { o.ptr = nullptr; o.bytes = 0; }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) { release(); ptr = o.ptr; bytes = o.bytes; o.ptr = nullptr; o.bytes = 0; }
+    return *this;
+  }
+  ~DevBuf() { release(); }
+  void alloc(size_t b) {
+    release();
+    if (b) IMPS_CUDA(cudaMalloc(&ptr, b));
+    bytes = b;
+  }
+  // Grow-only: keeps the allocation when it is already large enough.
+  void ensure(size_t b) { if (b > bytes) alloc(b); }
+  void release() { if (ptr) cudaFree(ptr); ptr = nullptr; bytes = 0; }
+  dcplx* z() const { return static_cast<dcplx*>(ptr); }
+  double* d() const { return static_cast<double*>(ptr); }
+};
+
+// Kernel timing accumulated per kernel class (CUDA events on the context stream).
+struct KernelStat {
+  int64_t launches = 0;
+  double ms = 0.0;
+  double flops = 0.0;   // algorithmic flops (or bytes for memory-bound kernels)
+};
+
+enum GemmPrecision { PREC_FP64 = 0, PREC_SPLIT_I8 = 1 };
+
+struct Context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = true;
+  cusolverDnHandle_t solver = nullptr;
+  int precision = PREC_FP64;
+  int nslices = 5;           // int8 slices per operand in split mode
+  bool adaptive_slices = false;
+  std::string last_error;
+  // named grow-only scratch buffers
+  std::map<std::string, DevBuf> scratch;
+  // reduction scratch (per-block partials) and pinned host staging
+  DevBuf red;
+  double* host_pinned = nullptr;
+  size_t host_pinned_bytes = 0;
+  int* dev_info = nullptr;
+  // profiling
+  bool profile = false;
+  std::map<std::string, KernelStat> stats;
+  std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
+  double pending_flops_dummy = 0;
+  std::vector<double> pending_flops;
+  // counters
+  int64_t n_ac_apply = 0, n_c_apply = 0, n_push = 0, n_gemm = 0, n_kernels = 0;
+  int num_sms = 148;
+
+  DevBuf& buf(const std::string& name, size_t bytes) {
+    DevBuf& b = scratch[name];
+    b.ensure(bytes);
+    return b;
+  }
+  double* pinned(size_t bytes);
+};
+
+// RAII timer for one kernel class on the context stream (active when profiling).
+struct ScopedTimer {
+  Context* ctx;
+  std::string name;
+  double flops;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  ScopedTimer(Context* c, const char* n, double f);
+  ~ScopedTimer();
+};
+
+// ---------------------------------------------------------------------------
+// Objects behind the opaque ABI handles
+// ---------------------------------------------------------------------------
+struct MpoSite {
+  int m = 0, d = 0, n = 0;       // left levels, physical dim, right levels
+  std::vector<cplx> W;           // dense (m, d, n, d), column-major
+  DevBuf Wdev;                   // same on device
+  // nonzero (i, j) blocks, 0-based
+  std::vector<std::pair<int, int>> nz;
+  bool block_nonzero(int i, int j) const;
+  cplx at(int i, int u, int j, int s) const { return W[i + (size_t)m * (u + (size_t)d * (j + (size_t)n * s))]; }
+};
+
+}  // namespace imps
+
+struct imps_mpo {
+  imps::Context* ctx;
+  int N;
+  std::vector<imps::MpoSite> sites;
+  std::vector<imps::MpoSite> closing;  // closing column (m, d, 1, d) of each site, for the Schur energy
+  bool isidentitylevel(int i) const;  // 1-based level label
+  bool isemptylevel(int i) const;
+};
+
+struct imps_state {
+  imps::Context* ctx;
+  int N;
+  std::vector<int> d;     // physical dim per site
+  std::vector<int> chi;   // chi[l] = bond dimension right of site l (bond N-1 == bond 0)
+  std::vector<imps::DevBuf> AL, AR, C, AC;
+  int Dl(int l) const { return chi[((l - 1) % N + N) % N]; }
+  int Dr(int l) const { return chi[((l % N) + N) % N]; }
+  size_t site_elems(int l) const { return (size_t)Dl(l) * d[l] * Dr(l); }
+  size_t bond_elems(int l) const { return (size_t)Dr(l) * Dr(l); }
+};
+
+struct imps_envs {
+  imps::Context* ctx;
+  int N;
+  std::vector<int> Dl, Dr, ml, nr;
+  std::vector<imps::DevBuf> lefts, rights;   // (Dl, ml, Dl), (Dr, nr, Dr)
+  // previous environments kept as the warm start of the next build
+  std::vector<imps::DevBuf> init_lefts, init_rights;
+  // Permuted copy of the left environment used by the C Hamiltonian:
+  // GLp[l][a + D (a' + D w)] = lefts[l][a, w, a'].  Rebuilt lazily.
+  std::vector<imps::DevBuf> GLp;
+  std::vector<bool> GLp_valid;
+  int64_t version = 0;
+  imps_env_info last;
+};
+
+namespace imps {
+
+// ---------------------------------------------------------------------------
+// Kernels / building blocks (defined in the .cu files)
+// ---------------------------------------------------------------------------
+enum Op { OP_N = 0, OP_T = 1, OP_C = 2 };
+
+// Column-major complex GEMM: C = alpha op(A) op(B) + beta C, batched with strides
+// (in complex elements).  Dispatches on ctx->precision for the large products.
+void zgemm(Context* ctx, Op opA, Op opB, int M, int N, int K, cplx alpha, const dcplx* A, int64_t lda,
+           int64_t strideA, const dcplx* B, int64_t ldb, int64_t strideB, cplx beta, dcplx* C, int64_t ldc,
+           int64_t strideC, int batch, bool allow_split = true);
+// Always the FP64 engine.
+void zgemm_fp64(Context* ctx, Op opA, Op opB, int M, int N, int K, cplx alpha, const dcplx* A, int64_t lda,
+                int64_t strideA, const dcplx* B, int64_t ldb, int64_t strideB, cplx beta, dcplx* C,
+                int64_t ldc, int64_t strideC, int batch);
+
+// Strided block-sparse level mixing (the MPO contraction between the GEMMs):
+// out[b,p,q,c] = sum_{(r,q) in nz} sum_s M[r,p,q,s] in[b,r,s,c], b contiguous.
+struct MixPlan {
+  int Db, P, S, C;            // extents of b, p (out phys), s (in phys), c
+  int R, Q;                   // extents of r (in level) and q (out level)
+  int64_t in_r, in_s, in_c;   // input strides (b stride = 1)
+  int64_t out_p, out_q, out_c;
+  const dcplx* M;             // dense (R, P, Q, S) column-major
+  std::vector<std::pair<int, int>> nz;  // (r, q) nonzero blocks
+  cplx scale = cplx(1.0, 0.0);
+};
+void level_mix(Context* ctx, const MixPlan& plan, const dcplx* in, dcplx* out);
+
+// BLAS-1 style helpers (deterministic two-pass reductions)
+void zcopy(Context* ctx, int64_t n, const dcplx* x, dcplx* y);
+void zscal(Context* ctx, int64_t n, cplx a, dcplx* x);
+void zaxpy(Context* ctx, int64_t n, cplx a, const dcplx* x, dcplx* y);        // y += a x
+void zaxpby(Context* ctx, int64_t n, cplx a, const dcplx* x, cplx b, dcplx* y); // y = a x + b y
+void zfill(Context* ctx, int64_t n, cplx v, dcplx* x);
+void zset_identity(Context* ctx, int D, dcplx* X, int64_t ld, cplx diag);
+double dznrm2(Context* ctx, int64_t n, const dcplx* x);
+cplx zdotc(Context* ctx, int64_t n, const dcplx* x, const dcplx* y);  // sum conj(x) y
+// h[j] = sum_k conj(V[k + ldv j]) w[k], j < nv  (one fused pass over V)
+void zdotc_multi(Context* ctx, int64_t n, int nv, const dcplx* V, int64_t ldv, const dcplx* w, cplx* h_host);
+// w += sum_j coef[j] V[:, j]
+void zgemv_acc(Context* ctx, int64_t n, int nv, const dcplx* V, int64_t ldv, const cplx* coef, dcplx* w);
+// y = sum_j coef[j] V[:, j]
+void zgemv_set(Context* ctx, int64_t n, int nv, const dcplx* V, int64_t ldv, const cplx* coef, dcplx* y);
+// X (m x n, ldx) -> Y = X^H (n x m, ldy)
+void zconj_transpose(Context* ctx, int m, int n, const dcplx* X, int64_t ldx, dcplx* Y, int64_t ldy);
+// trace(L * V) with L, V  D x D (regularize! coefficient, sum L[a,b] V[b,a])
+cplx ztrace_prod(Context* ctx, int D, const dcplx* L, int64_t ldl, const dcplx* V, int64_t ldv);
+void zadd_diag(Context* ctx, int D, dcplx* X, int64_t ld, cplx v);
+void zfill2d(Context* ctx, int rows, int cols, cplx v, dcplx* Y, int64_t ldy);
+// X[:, lvl-slice] strided copy helpers
+void zcopy2d(Context* ctx, int rows, int cols, const dcplx* X, int64_t ldx, dcplx* Y, int64_t ldy);
+void zadd2d(Context* ctx, int rows, int cols, const dcplx* X, int64_t ldx, dcplx* Y, int64_t ldy);
+
+// Orthogonal factorizations with a non-negative real diagonal (QRpos / LQpos).
+// Q overwrites nothing: results go to Q (m x k) and R (k x n), k = min(m, n).
+void qrpos(Context* ctx, int m, int n, const dcplx* M, int64_t ldm, dcplx* Q, dcplx* R);
+void lqpos(Context* ctx, int m, int n, const dcplx* M, int64_t ldm, dcplx* L, dcplx* Q);
+
+// Host <-> device
+void upload(Context* ctx, void* dst, const void* src, size_t bytes);
+void download(Context* ctx, void* dst, const void* src, size_t bytes);
+
+// ---------------------------------------------------------------------------
+// Tensor-network operations (heff.cu)
+// ---------------------------------------------------------------------------
+// AC effective Hamiltonian y = H_AC x for site `site` (0-based); `Wover` optionally
+// replaces the site's MPO tensor (used for the closing-column energy).
+void ac_apply(Context* ctx, const imps_envs* envs, const imps_mpo* mpo, int site, const dcplx* x, dcplx* y,
+              const MpoSite* Wover = nullptr, const dcplx* GRover = nullptr, int64_t GRover_ld = 0);
+void c_apply(Context* ctx, imps_envs* envs, int site, const dcplx* x, dcplx* y);
+// identity-channel pushes with distinct above/below tensors (transfermatrix.jl:5-66)
+void push_left_id(Context* ctx, int Dl, int d, int Dr, const dcplx* L, const dcplx* above, const dcplx* below,
+                  dcplx* out);
+void push_right_id(Context* ctx, int Dl, int d, int Dr, const dcplx* R, const dcplx* above, const dcplx* below,
+                   dcplx* out);
+// Level-resolved pushes: out_q = sum_{(l,q)} push_slice(L_l, W[l,:,q,:], A)
+void push_left_levels(Context* ctx, const MpoSite& W, int Dl, int d, int Dr, const dcplx* L, int64_t L_level_stride,
+                      int64_t L_ld, const std::vector<std::pair<int, int>>& blocks, int q_count,
+                      const std::vector<int>& q_targets, const dcplx* A, dcplx* out, int64_t out_level_stride,
+                      int64_t out_ld, bool accumulate);
+void push_right_levels(Context* ctx, const MpoSite& W, int Dl, int d, int Dr, const dcplx* R,
+                       int64_t R_level_stride, int64_t R_ld, const std::vector<std::pair<int, int>>& blocks,
+                       const std::vector<int>& q_targets, const dcplx* A, dcplx* out, int64_t out_level_stride,
+                       int64_t out_ld, bool accumulate);
+// Full MPO pushes (transfer_leftenv!/transfer_rightenv!)
+void push_mpo_left(Context* ctx, const MpoSite& W, int Dl, int d, int Dr, const dcplx* L, const dcplx* A, dcplx* out);
+void push_mpo_right(Context* ctx, const MpoSite& W, int Dl, int d, int Dr, const dcplx* R, const dcplx* A,
+                    dcplx* out);
+
+}  // namespace imps

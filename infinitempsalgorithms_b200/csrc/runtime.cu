@@ -1,0 +1,443 @@
+// Context, transfers, timing and the memory-bound vector kernels (Krylov
+// orthogonalisation, norms, axpy, transposes).  Reductions are two-pass and
+// deterministic: per-block partials in a fixed order, then one final block.
+#include "imps_internal.h"
+
+#include <algorithm>
+#include <cstring>
+
+namespace imps {
+
+namespace {
+constexpr int kRedThreads = 256;
+constexpr int kMaxRedBlocks = 1184;  // 8 x 148 SMs
+
+__device__ __forceinline__ dcplx cmul(dcplx a, dcplx b) {
+  return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ dcplx cmulc(dcplx a, dcplx b) {  // conj(a) * b
+  return make_double2(fma(a.x, b.x, a.y * b.y), fma(a.x, b.y, -a.y * b.x));
+}
+
+int red_blocks(int64_t n) {
+  int64_t b = (n + kRedThreads - 1) / kRedThreads;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(b, kMaxRedBlocks));
+}
+
+template <int NT>
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < NT / 32; ++i) r += sh[i];
+  }
+  __syncthreads();
+  return r;
+}
+
+__global__ void k_nrm2_partial(int64_t n, const dcplx* __restrict__ x, double* __restrict__ part) {
+  __shared__ double sh[kRedThreads / 32];
+  double s = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    dcplx v = x[i];
+    s = fma(v.x, v.x, fma(v.y, v.y, s));
+  }
+  double r = block_sum<kRedThreads>(s, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = r;
+}
+
+__global__ void k_dotc_partial(int64_t n, const dcplx* __restrict__ x, const dcplx* __restrict__ y,
+                               double* __restrict__ part) {
+  __shared__ double sh[kRedThreads / 32];
+  double sr = 0.0, si = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    dcplx p = cmulc(x[i], y[i]);
+    sr += p.x;
+    si += p.y;
+  }
+  double r = block_sum<kRedThreads>(sr, sh);
+  double q = block_sum<kRedThreads>(si, sh);
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = r;
+    part[2 * blockIdx.x + 1] = q;
+  }
+}
+
+// Sum `ncol` columns of partials (each `nb` long, stride ld) in a fixed order.
+__global__ void k_final_sum(int nb, int ncol, const double* __restrict__ part, int64_t ld, double* __restrict__ out) {
+  __shared__ double sh[kRedThreads / 32];
+  for (int c = 0; c < ncol; ++c) {
+    double s = 0.0;
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) s += part[i + ld * c];
+    double r = block_sum<kRedThreads>(s, sh);
+    if (threadIdx.x == 0) out[c] = r;
+  }
+}
+
+// h[j] partials for a chunk of up to 8 basis vectors.
+template <int CH>
+__global__ void k_dotc_multi_partial(int64_t n, int nv, const dcplx* __restrict__ V, int64_t ldv,
+                                     const dcplx* __restrict__ w, double* __restrict__ part, int64_t ldp) {
+  __shared__ double sh[kRedThreads / 32];
+  double ar[CH], ai[CH];
+#pragma unroll
+  for (int j = 0; j < CH; ++j) { ar[j] = 0.0; ai[j] = 0.0; }
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    dcplx wi = w[i];
+#pragma unroll
+    for (int j = 0; j < CH; ++j) {
+      if (j < nv) {
+        dcplx p = cmulc(V[i + ldv * j], wi);
+        ar[j] += p.x;
+        ai[j] += p.y;
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < CH; ++j) {
+    if (j < nv) {
+      double r = block_sum<kRedThreads>(ar[j], sh);
+      double q = block_sum<kRedThreads>(ai[j], sh);
+      if (threadIdx.x == 0) {
+        part[blockIdx.x + ldp * (2 * j)] = r;
+        part[blockIdx.x + ldp * (2 * j + 1)] = q;
+      }
+    }
+  }
+}
+
+struct CoefPack {
+  double2 c[32];
+};
+
+__global__ void k_gemv_acc(int64_t n, int nv, const dcplx* __restrict__ V, int64_t ldv, CoefPack coef,
+                           dcplx* __restrict__ w, int set) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    dcplx acc = set ? make_double2(0.0, 0.0) : w[i];
+    for (int j = 0; j < nv; ++j) {
+      dcplx p = cmul(coef.c[j], V[i + ldv * j]);
+      acc.x += p.x;
+      acc.y += p.y;
+    }
+    w[i] = acc;
+  }
+}
+
+__global__ void k_scal(int64_t n, double2 a, dcplx* x) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    x[i] = cmul(a, x[i]);
+}
+__global__ void k_axpby(int64_t n, double2 a, const dcplx* __restrict__ x, double2 b, dcplx* __restrict__ y,
+                        int use_b) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    dcplx v = cmul(a, x[i]);
+    if (use_b) {
+      dcplx u = cmul(b, y[i]);
+      v.x += u.x;
+      v.y += u.y;
+    }
+    y[i] = v;
+  }
+}
+__global__ void k_axpy(int64_t n, double2 a, const dcplx* __restrict__ x, dcplx* __restrict__ y) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    dcplx v = cmul(a, x[i]);
+    dcplx u = y[i];
+    y[i] = make_double2(u.x + v.x, u.y + v.y);
+  }
+}
+__global__ void k_fill(int64_t n, double2 v, dcplx* x) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    x[i] = v;
+}
+__global__ void k_set_identity(int D, dcplx* X, int64_t ld, double2 diag) {
+  int64_t total = (int64_t)D * D;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    int a = (int)(t % D), b = (int)(t / D);
+    X[a + ld * b] = (a == b) ? diag : make_double2(0.0, 0.0);
+  }
+}
+
+// 32 x 32 tiled conjugate transpose: Y[j + ldy i] = conj(X[i + ldx j]).
+__global__ void k_conj_transpose(int m, int n, const dcplx* __restrict__ X, int64_t ldx, dcplx* __restrict__ Y,
+                                 int64_t ldy) {
+  __shared__ dcplx tile[32][33];
+  int i0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    int i = i0 + threadIdx.x, j = j0 + r;
+    if (i < m && j < n) tile[r][threadIdx.x] = X[i + ldx * j];
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    int j = j0 + threadIdx.x, i = i0 + r;
+    if (i < m && j < n) {
+      dcplx v = tile[threadIdx.x][r];
+      Y[j + ldy * i] = make_double2(v.x, -v.y);
+    }
+  }
+}
+
+// partials of sum_{a,b} L[a,b] V[b,a]
+__global__ void k_trace_prod_partial(int D, const dcplx* __restrict__ L, int64_t ldl, const dcplx* __restrict__ V,
+                                     int64_t ldv, double* __restrict__ part) {
+  __shared__ double sh[kRedThreads / 32];
+  double sr = 0.0, si = 0.0;
+  int64_t total = (int64_t)D * D;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    int a = (int)(t % D), b = (int)(t / D);
+    dcplx p = cmul(L[a + ldl * b], V[b + ldv * a]);
+    sr += p.x;
+    si += p.y;
+  }
+  double r = block_sum<kRedThreads>(sr, sh);
+  double q = block_sum<kRedThreads>(si, sh);
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = r;
+    part[2 * blockIdx.x + 1] = q;
+  }
+}
+
+__global__ void k_copy2d(int rows, int cols, const dcplx* __restrict__ X, int64_t ldx, dcplx* __restrict__ Y,
+                         int64_t ldy, int add) {
+  int64_t total = (int64_t)rows * cols;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    int r = (int)(t % rows), c = (int)(t / rows);
+    dcplx v = X[r + ldx * c];
+    if (add) {
+      dcplx u = Y[r + ldy * c];
+      v.x += u.x;
+      v.y += u.y;
+    }
+    Y[r + ldy * c] = v;
+  }
+}
+
+__global__ void k_add_diag(int D, dcplx* X, int64_t ld, double2 v) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < D; i += gridDim.x * blockDim.x) {
+    dcplx u = X[i + ld * i];
+    X[i + ld * i] = make_double2(u.x + v.x, u.y + v.y);
+  }
+}
+__global__ void k_fill2d(int rows, int cols, dcplx* Y, int64_t ldy, double2 v) {
+  int64_t total = (int64_t)rows * cols;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    int r = (int)(t % rows), c = (int)(t / rows);
+    Y[r + ldy * c] = v;
+  }
+}
+
+int grid_for(int64_t n, int threads = 256) {
+  int64_t b = (n + threads - 1) / threads;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(b, 148 * 16));
+}
+
+inline double2 d2(cplx z) { return make_double2(z.real(), z.imag()); }
+
+void check_launch(Context* ctx) {
+  ctx->n_kernels++;
+  cudaError_t e = cudaPeekAtLastError();
+  if (e != cudaSuccess) throw Error(IMPS_CUDA_ERROR, std::string("kernel launch: ") + cudaGetErrorString(e));
+}
+
+}  // namespace
+
+double* Context::pinned(size_t bytes) {
+  if (bytes > host_pinned_bytes) {
+    if (host_pinned) cudaFreeHost(host_pinned);
+    host_pinned = nullptr;
+    size_t b = std::max<size_t>(bytes, 1 << 16);
+    IMPS_CUDA(cudaMallocHost((void**)&host_pinned, b));
+    host_pinned_bytes = b;
+  }
+  return host_pinned;
+}
+
+ScopedTimer::ScopedTimer(Context* c, const char* n, double f) : ctx(c), name(n), flops(f) {
+  if (ctx->profile) {
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, ctx->stream);
+  }
+}
+ScopedTimer::~ScopedTimer() {
+  if (ctx->profile && e0) {
+    cudaEventRecord(e1, ctx->stream);
+    ctx->pending.push_back({name, {e0, e1}});
+    ctx->pending_flops.push_back(flops);
+  }
+}
+
+void upload(Context* ctx, void* dst, const void* src, size_t bytes) {
+  if (!bytes) return;
+  IMPS_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  IMPS_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+void download(Context* ctx, void* dst, const void* src, size_t bytes) {
+  if (!bytes) return;
+  IMPS_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  IMPS_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
+void zcopy(Context* ctx, int64_t n, const dcplx* x, dcplx* y) {
+  if (n <= 0 || x == y) return;
+  IMPS_CUDA(cudaMemcpyAsync(y, x, n * sizeof(dcplx), cudaMemcpyDeviceToDevice, ctx->stream));
+}
+void zscal(Context* ctx, int64_t n, cplx a, dcplx* x) {
+  if (n <= 0) return;
+  k_scal<<<grid_for(n), 256, 0, ctx->stream>>>(n, d2(a), x);
+  check_launch(ctx);
+}
+void zaxpy(Context* ctx, int64_t n, cplx a, const dcplx* x, dcplx* y) {
+  if (n <= 0) return;
+  k_axpy<<<grid_for(n), 256, 0, ctx->stream>>>(n, d2(a), x, y);
+  check_launch(ctx);
+}
+void zaxpby(Context* ctx, int64_t n, cplx a, const dcplx* x, cplx b, dcplx* y) {
+  if (n <= 0) return;
+  k_axpby<<<grid_for(n), 256, 0, ctx->stream>>>(n, d2(a), x, d2(b), y, b != cplx(0.0, 0.0));
+  check_launch(ctx);
+}
+void zfill(Context* ctx, int64_t n, cplx v, dcplx* x) {
+  if (n <= 0) return;
+  k_fill<<<grid_for(n), 256, 0, ctx->stream>>>(n, d2(v), x);
+  check_launch(ctx);
+}
+void zset_identity(Context* ctx, int D, dcplx* X, int64_t ld, cplx diag) {
+  if (D <= 0) return;
+  k_set_identity<<<grid_for((int64_t)D * D), 256, 0, ctx->stream>>>(D, X, ld, d2(diag));
+  check_launch(ctx);
+}
+
+double dznrm2(Context* ctx, int64_t n, const dcplx* x) {
+  if (n <= 0) return 0.0;
+  int nb = red_blocks(n);
+  DevBuf& red = ctx->buf("red_part", (size_t)(nb + 8) * sizeof(double));
+  DevBuf& out = ctx->buf("red_out", 64 * sizeof(double));
+  ScopedTimer t(ctx, "blas1", (double)n * 16);
+  k_nrm2_partial<<<nb, kRedThreads, 0, ctx->stream>>>(n, x, red.d());
+  check_launch(ctx);
+  k_final_sum<<<1, kRedThreads, 0, ctx->stream>>>(nb, 1, red.d(), nb, out.d());
+  check_launch(ctx);
+  double h;
+  download(ctx, &h, out.d(), sizeof(double));
+  return std::sqrt(h);
+}
+
+cplx zdotc(Context* ctx, int64_t n, const dcplx* x, const dcplx* y) {
+  if (n <= 0) return cplx(0.0, 0.0);
+  int nb = red_blocks(n);
+  DevBuf& red = ctx->buf("red_part", (size_t)(2 * nb + 8) * sizeof(double));
+  DevBuf& out = ctx->buf("red_out", 64 * sizeof(double));
+  ScopedTimer t(ctx, "blas1", (double)n * 32);
+  (void)out;
+  k_dotc_partial<<<nb, kRedThreads, 0, ctx->stream>>>(n, x, y, red.d());
+  check_launch(ctx);
+  double h[2];
+  {
+    // per-block (re, im) partials summed on the host in block order (deterministic)
+    std::vector<double> p(2 * nb);
+    download(ctx, p.data(), red.d(), p.size() * sizeof(double));
+    double sr = 0.0, si = 0.0;
+    for (int i = 0; i < nb; ++i) { sr += p[2 * i]; si += p[2 * i + 1]; }
+    h[0] = sr;
+    h[1] = si;
+  }
+  return cplx(h[0], h[1]);
+}
+
+void zdotc_multi(Context* ctx, int64_t n, int nv, const dcplx* V, int64_t ldv, const dcplx* w, cplx* h_host) {
+  if (nv <= 0) return;
+  int nb = std::min(red_blocks(n), 592);
+  constexpr int CH = 8;
+  int nchunks = (nv + CH - 1) / CH;
+  DevBuf& red = ctx->buf("red_multi", (size_t)nb * 2 * CH * nchunks * sizeof(double));
+  DevBuf& out = ctx->buf("red_multi_out", (size_t)2 * CH * nchunks * sizeof(double));
+  ScopedTimer t(ctx, "orth", (double)n * 16 * (nv + 1));
+  for (int c = 0; c < nchunks; ++c) {
+    int nvc = std::min(CH, nv - c * CH);
+    k_dotc_multi_partial<CH><<<nb, kRedThreads, 0, ctx->stream>>>(n, nvc, V + ldv * (int64_t)(c * CH), ldv, w,
+                                                                  red.d() + (size_t)nb * 2 * CH * c, nb);
+    check_launch(ctx);
+  }
+  k_final_sum<<<1, kRedThreads, 0, ctx->stream>>>(nb, 2 * CH * nchunks, red.d(), nb, out.d());
+  check_launch(ctx);
+  std::vector<double> hv(2 * CH * nchunks);
+  download(ctx, hv.data(), out.d(), hv.size() * sizeof(double));
+  for (int j = 0; j < nv; ++j) {
+    int c = j / CH, jj = j % CH;
+    h_host[j] = cplx(hv[2 * CH * c + 2 * jj], hv[2 * CH * c + 2 * jj + 1]);
+  }
+}
+
+static void gemv_common(Context* ctx, int64_t n, int nv, const dcplx* V, int64_t ldv, const cplx* coef, dcplx* w,
+                        int set) {
+  ScopedTimer t(ctx, "orth", (double)n * 16 * (nv + 2));
+  int done = 0;
+  bool first = true;
+  while (done < nv || (first && set)) {
+    int cnt = std::min(32, nv - done);
+    CoefPack p;
+    for (int j = 0; j < cnt; ++j) p.c[j] = d2(coef[done + j]);
+    k_gemv_acc<<<grid_for(n), 256, 0, ctx->stream>>>(n, cnt, V + ldv * (int64_t)done, ldv, p, w,
+                                                      (first && set) ? 1 : 0);
+    check_launch(ctx);
+    done += cnt;
+    first = false;
+    if (cnt == 0) break;
+  }
+}
+void zgemv_acc(Context* ctx, int64_t n, int nv, const dcplx* V, int64_t ldv, const cplx* coef, dcplx* w) {
+  if (nv <= 0) return;
+  gemv_common(ctx, n, nv, V, ldv, coef, w, 0);
+}
+void zgemv_set(Context* ctx, int64_t n, int nv, const dcplx* V, int64_t ldv, const cplx* coef, dcplx* y) {
+  gemv_common(ctx, n, nv, V, ldv, coef, y, 1);
+}
+
+void zconj_transpose(Context* ctx, int m, int n, const dcplx* X, int64_t ldx, dcplx* Y, int64_t ldy) {
+  if (m <= 0 || n <= 0) return;
+  dim3 grid((m + 31) / 32, (n + 31) / 32), block(32, 8);
+  ScopedTimer t(ctx, "permute", (double)m * n * 32);
+  k_conj_transpose<<<grid, block, 0, ctx->stream>>>(m, n, X, ldx, Y, ldy);
+  check_launch(ctx);
+}
+
+cplx ztrace_prod(Context* ctx, int D, const dcplx* L, int64_t ldl, const dcplx* V, int64_t ldv) {
+  int64_t n = (int64_t)D * D;
+  int nb = red_blocks(n);
+  DevBuf& red = ctx->buf("red_part", (size_t)(2 * nb + 8) * sizeof(double));
+  k_trace_prod_partial<<<nb, kRedThreads, 0, ctx->stream>>>(D, L, ldl, V, ldv, red.d());
+  check_launch(ctx);
+  std::vector<double> p(2 * nb);
+  download(ctx, p.data(), red.d(), p.size() * sizeof(double));
+  double sr = 0.0, si = 0.0;
+  for (int i = 0; i < nb; ++i) { sr += p[2 * i]; si += p[2 * i + 1]; }
+  return cplx(sr, si);
+}
+
+void zcopy2d(Context* ctx, int rows, int cols, const dcplx* X, int64_t ldx, dcplx* Y, int64_t ldy) {
+  if (rows <= 0 || cols <= 0) return;
+  k_copy2d<<<grid_for((int64_t)rows * cols), 256, 0, ctx->stream>>>(rows, cols, X, ldx, Y, ldy, 0);
+  check_launch(ctx);
+}
+void zadd2d(Context* ctx, int rows, int cols, const dcplx* X, int64_t ldx, dcplx* Y, int64_t ldy) {
+  if (rows <= 0 || cols <= 0) return;
+  k_copy2d<<<grid_for((int64_t)rows * cols), 256, 0, ctx->stream>>>(rows, cols, X, ldx, Y, ldy, 1);
+  check_launch(ctx);
+}
+
+void zadd_diag(Context* ctx, int D, dcplx* X, int64_t ld, cplx v) {
+  if (D <= 0) return;
+  k_add_diag<<<grid_for(D), 256, 0, ctx->stream>>>(D, X, ld, d2(v));
+  check_launch(ctx);
+}
+void zfill2d(Context* ctx, int rows, int cols, cplx v, dcplx* Y, int64_t ldy) {
+  if (rows <= 0 || cols <= 0) return;
+  k_fill2d<<<grid_for((int64_t)rows * cols), 256, 0, ctx->stream>>>(rows, cols, Y, ldy, d2(v));
+  check_launch(ctx);
+}
+
+}  // namespace imps

@@ -1,0 +1,14 @@
+// Small dense FP64 eigenproblems used by the Krylov solvers (see smallla.cu).
+#pragma once
+#include <complex>
+#include <vector>
+
+namespace imps {
+using cplx = std::complex<double>;
+// Hermitian n x n (column-major) -> ascending eigenvalues w, eigenvectors V (columns).
+void herm_eig(int n, const std::vector<cplx>& A, std::vector<double>& w, std::vector<cplx>& V);
+// General n x n (column-major) -> eigenvalues lam, unit eigenvectors Y (columns).
+void gen_eig(int n, const std::vector<cplx>& H, std::vector<cplx>& lam, std::vector<cplx>& Y);
+// exp(t Hs) e1 for a Hermitian m x m matrix.
+void herm_expm_e1(int m, const std::vector<cplx>& Hs, cplx t, std::vector<cplx>& out);
+}  // namespace imps

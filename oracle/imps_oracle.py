@@ -1,0 +1,1360 @@
+"""NumPy/SciPy restatement of the InfiniteMPSAlgorithms VUMPS/TDVP inner loop.
+
+TEST INFRASTRUCTURE ONLY -- the oracle.  It is imported by ``tests/``,
+``__graft_entry__.smoke()`` and the CPU-baseline legs of ``bench.py``, and by
+nothing that ships.  The product path (``infinitempsalgorithms_b200``) never
+calls it.
+
+Parity status
+-------------
+* The reference is pure Julia and cannot run in this container (no ``julia``,
+  and its dependencies KrylovKit / TensorOperations / FiniteMPSAlgorithms are
+  absent).  Every function below restates the cited reference lines.
+* Pinned against the reference's own known-answer tests (``tests/test_oracle.py``):
+  TFIM ``e0 = -4/pi`` (``test/algorithms/vumps.jl:15-18``), XXZ
+  ``e0 = 1/4 - ln 2`` (``vumps.jl:7-12``), the N=1 TFIM Galerkin < 1e-9 run
+  (``test/algorithms/api.jl:481-489``), Heff Hermiticity and identity
+  (``api.jl:226-239``), ``regularize!`` (``api.jl:243-246``), ``linsolve``
+  coefficients (``api.jl:248-251``), ``contract_mpo_expval``
+  (``api.jl:253-257``), ``DynamicTol`` (``api.jl:453-462``), ``integrate``
+  (``api.jl:469-478``) and the TDVP conservation laws (``test/algorithms/tdvp.jl:14-24``).
+* KrylovKit internals (restart policy, Ritz-vector phase) are UNPINNED: the
+  library is absent.  The Krylov solvers below restate the published
+  algorithms (thick-restart Lanczos, restarted GMRES with Givens rotations,
+  Krylov exponential with sub-stepping, Arnoldi with Ritz restart); the CUDA
+  runtime implements exactly the same algorithms, so the trajectories agree.
+
+Conventions (identical to the reference, Julia column-major)
+-------------------------------------------------------------
+* site tensors ``A[a, s, b]`` of shape ``(Dl, d, Dr)``;
+* left environments ``GL[bra, level, ket]``, right ``GR[ket, level, bra]``
+  (``src/algorithms/groundstates/effective.jl:3-5``);
+* dense MPO tensors ``W[wl, u, wr, s]`` with ``u`` the output (bra) leg
+  (``envs.jl:332``, ``tompotensor``);
+* all arrays are kept in Fortran order and reshaped with ``order='F'`` so each
+  reshape is the reference's ``reshape``.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import Callable, List, Optional, Sequence
+
+import numpy as np
+
+__all__ = [
+    "freshape", "fzeros", "C128", "Defaults", "DynamicTol", "alg_eigsolve", "alg_gauge",
+    "alg_environments", "alg_expsolve", "canonical_from_AL", "canonical_from_sites",
+    "canonical_from_AL_keepAL", "_mulAL", "_mulCA", "hubbard_operators", "updatetol", "sigma", "spin", "mpohamiltonian",
+    "SchurMPO", "tfim_hamiltonian", "heisenberg_hamiltonian", "hubbard_hamiltonian",
+    "tfim_e0", "hubbard_e0", "qrpos", "lqpos", "lanczos_eigsolve", "gmres",
+    "exponentiate", "arnoldi_dominant", "KrylovInfo", "push_env_left",
+    "push_env_right", "push_slice_left", "push_slice_right", "push_mpo_left",
+    "push_mpo_right", "regularize", "CanonicalIMPS", "uniform_leftorth",
+    "uniform_rightorth", "gaugefix", "regauge", "randomimps", "random_site_tensors",
+    "state_dot", "DMRGCache", "build_envs", "ac_apply", "c_apply", "calc_galerkin",
+    "expectationvalue", "local_expectation1", "VUMPS", "TDVP", "IDMRG",
+    "find_groundstate", "timestep", "time_evolve", "idmrg_groundstate",
+]
+
+C128 = np.complex128
+
+
+def freshape(x, shape):
+    return np.reshape(x, shape, order="F")
+
+
+def fzeros(shape, dtype=C128):
+    return np.zeros(shape, dtype=dtype, order="F")
+
+
+# --------------------------------------------------------------------------
+# Defaults and DynamicTol  (src/utility.jl:136-171, 297-365)
+# --------------------------------------------------------------------------
+class Defaults:
+    """Mirror of ``module Defaults`` (``src/utility.jl:297-365``)."""
+    D = 64
+    maxiter = 300
+    tolgauge = 1.0e-13
+    tol = 1.0e-10
+    verbosity = 0
+    krylovdim = 30
+    dynamic_tols = True
+    tol_min = 1.0e-14
+    tol_max = 1.0e-4
+    eigs_tolfactor = 1.0e-3
+    gauge_tolfactor = 1.0e-6
+    envs_tolfactor = 1.0e-4
+
+
+@dataclass
+class DynamicTol:
+    """``DynamicTol(alg, tol_min, tol_max, tol_factor)`` (``src/utility.jl:136-148``).
+
+    ``alg`` is a dict with at least ``tol`` and ``maxiter``.
+    """
+    alg: dict
+    tol_min: float = 1.0e-6
+    tol_max: float = 1.0e-2
+    tol_factor: float = 0.1
+
+    def __post_init__(self):
+        if not (0 <= self.tol_min <= self.tol_max):
+            raise ValueError("DynamicTol requires 0 <= tol_min <= tol_max")
+
+
+def updatetol(alg, it: int, eps: float):
+    """``updatetol`` (``src/utility.jl:151-157``): clamp(eps*f/sqrt(iter), min, max)."""
+    if not isinstance(alg, DynamicTol):
+        return alg
+    it = max(it, 1)
+    new_tol = min(max(eps * alg.tol_factor / math.sqrt(it), alg.tol_min), alg.tol_max)
+    out = dict(alg.alg)
+    out["tol"] = new_tol
+    return out
+
+
+def alg_eigsolve(tol=Defaults.tol, maxiter=Defaults.maxiter, krylovdim=Defaults.krylovdim,
+                 eager=True, tol_factor=Defaults.eigs_tolfactor, dynamic=True):
+    """``Defaults.alg_eigsolve`` (``src/utility.jl:330-340``)."""
+    alg = dict(tol=tol, maxiter=maxiter, krylovdim=krylovdim, eager=eager)
+    return DynamicTol(alg, Defaults.tol_min, Defaults.tol_max, tol_factor) if dynamic else alg
+
+
+def alg_gauge(tol=Defaults.tolgauge, maxiter=Defaults.maxiter, dynamic=True):
+    """``Defaults.alg_gauge`` (``src/utility.jl:349-353``)."""
+    alg = dict(tol=tol, maxiter=maxiter)
+    return DynamicTol(alg, Defaults.tol_min, Defaults.tol_max, Defaults.gauge_tolfactor) if dynamic else alg
+
+
+def alg_environments(tol=Defaults.tol, maxiter=Defaults.maxiter, dynamic=True):
+    """``Defaults.alg_environments`` (``src/utility.jl:358-364``)."""
+    alg = dict(tol=tol, maxiter=maxiter)
+    return DynamicTol(alg, Defaults.tol_min, Defaults.tol_max, Defaults.envs_tolfactor) if dynamic else alg
+
+
+def alg_expsolve(tol=Defaults.tol, maxiter=Defaults.maxiter, krylovdim=Defaults.krylovdim):
+    """``Defaults.alg_expsolve`` (``src/utility.jl:343-347``)."""
+    return dict(tol=tol, maxiter=maxiter, krylovdim=krylovdim)
+
+
+# --------------------------------------------------------------------------
+# Models  (src/models.jl:61-122; Hubbard: own Jordan-Wigner construction)
+# --------------------------------------------------------------------------
+def sigma(which: str) -> np.ndarray:
+    """Pauli matrices (``src/models.jl:64-66``)."""
+    return {
+        "x": np.array([[0, 1], [1, 0]], dtype=C128),
+        "y": np.array([[0, -1j], [1j, 0]], dtype=C128),
+        "z": np.array([[1, 0], [0, -1]], dtype=C128),
+    }[which]
+
+
+def spin(which: str) -> np.ndarray:
+    """Spin-1/2 operators ``S = sigma/2`` (``src/models.jl:67-69``)."""
+    return sigma(which) / 2
+
+
+@dataclass
+class SchurMPO:
+    """A ``SparseIMPO`` (``src/operators/mpohamiltonian.jl:33-52``) as dense site tensors.
+
+    ``Ws[l]`` has shape ``(m, d, n, d)`` = ``tompotensor(H[l])`` (``envs.jl:332``):
+    ``W[i, u, j, s]`` is the ``(u_out, s_in)`` block from left level ``i`` to
+    right level ``j``; a structurally missing block is all zeros.
+    """
+    Ws: List[np.ndarray]
+
+    def __post_init__(self):
+        N = len(self.Ws)
+        if N == 0:
+            raise ValueError("Ws must not be empty")
+        for l in range(N):
+            l1 = (l + 1) % N
+            if self.Ws[l].shape[2] != self.Ws[l1].shape[0]:
+                raise ValueError("level chain mismatch")  # mpohamiltonian.jl:58-67
+        self.Ws = [np.asfortranarray(W, dtype=C128) for W in self.Ws]
+
+    def __len__(self):
+        return len(self.Ws)
+
+    def __getitem__(self, l):
+        return self.Ws[l % len(self.Ws)]
+
+    def space_l(self, l):
+        return self[l].shape[0]
+
+    def space_r(self, l):
+        return self[l].shape[2]
+
+    def block(self, l, i, j):
+        return self[l][i, :, j, :]
+
+    def isidentitylevel(self, i: int, atol=1e-14) -> bool:
+        """``isidentitylevel`` (``mpohamiltonian.jl:100-109``); ``i`` is 1-based."""
+        if i == 1:
+            return True
+        for W in self.Ws:
+            m, n = W.shape[0], W.shape[2]
+            if i == m == n:
+                continue
+            if i > m - 1 or i > n - 1:
+                return False
+            blk = W[i - 1, :, i - 1, :]
+            # isapprox(block, one(block); atol) with rtol = 0: Frobenius distance
+            if np.linalg.norm(blk - np.eye(blk.shape[0])) > atol:
+                return False
+        return True
+
+    def isemptylevel(self, i: int) -> bool:
+        """``isemptylevel`` (``mpohamiltonian.jl:122-133``); ``i`` is 1-based."""
+        if i == 1:
+            return False
+        if any(i == W.shape[2] for W in self.Ws):
+            return False
+        for W in self.Ws:
+            m, n = W.shape[0], W.shape[2]
+            dz = (i > m - 1 or i > n - 1) or not np.any(W[i - 1, :, i - 1, :])
+            cz = (i > n - 1) or not np.any(W[0, :, i - 1, :])
+            bz = (i > m - 1) or not np.any(W[i - 1, :, n - 1, :])
+            if not (dz and cz and bz):
+                return False
+        return True
+
+
+def mpohamiltonian(h1: np.ndarray, pairs: Sequence) -> np.ndarray:
+    """Schur level matrix -> dense ``(n, d, n, d)`` tensor (``src/models.jl:82-100``).
+
+    Levels 1 and n carry the identity, ``[1, n] = h1``, ``[1, k+1] = coeff_k a_k``
+    and ``[k+1, n] = b_k``; all other blocks are missing (zero).
+    """
+    d = h1.shape[0]
+    n = len(pairs) + 2
+    W = fzeros((n, d, n, d))
+    eye = np.eye(d, dtype=C128)
+    W[0, :, 0, :] = eye
+    W[n - 1, :, n - 1, :] = eye
+    W[0, :, n - 1, :] = h1
+    for k, (coeff, a, b) in enumerate(pairs):
+        W[0, :, k + 1, :] = coeff * np.asarray(a, dtype=C128)
+        W[k + 1, :, n - 1, :] = np.asarray(b, dtype=C128)
+    return W
+
+
+def tfim_hamiltonian(J=1.0, h=1.0) -> SchurMPO:
+    """``H = -J sum sx sx - h sum sz`` (``src/models.jl:119-122``), w = 3."""
+    return SchurMPO([mpohamiltonian(-h * sigma("z"), [(-J, sigma("x"), sigma("x"))])])
+
+
+def heisenberg_hamiltonian(J=1.0, Delta=1.0, h=0.0) -> SchurMPO:
+    """``H = J sum (SxSx + SySy + Delta SzSz) - h sum Sz`` (``src/models.jl:107-111``), w = 5."""
+    Sx, Sy, Sz = spin("x"), spin("y"), spin("z")
+    return SchurMPO([mpohamiltonian(-h * Sz, [(J, Sx, Sx), (J, Sy, Sy), (J * Delta, Sz, Sz)])])
+
+
+def hubbard_operators():
+    """Local fermion operators on ``(|0>, |up>, |dn>, |updn>)``, ``|updn> = c+_up c+_dn |0>``.
+
+    Returns ``(c_up, c_dn, P, n, n_updn)`` with ``P = (-1)^n`` the local parity.
+    """
+    c_up = np.zeros((4, 4), dtype=C128)
+    c_dn = np.zeros((4, 4), dtype=C128)
+    c_up[0, 1] = 1.0   # c_up |up>   = |0>
+    c_up[2, 3] = 1.0   # c_up |updn> = +|dn>
+    c_dn[0, 2] = 1.0   # c_dn |dn>   = |0>
+    c_dn[1, 3] = -1.0  # c_dn |updn> = -|up>
+    P = np.diag([1.0, -1.0, -1.0, 1.0]).astype(C128)
+    n = np.diag([0.0, 1.0, 1.0, 2.0]).astype(C128)
+    n_updn = np.diag([0.0, 0.0, 0.0, 1.0]).astype(C128)
+    return c_up, c_dn, P, n, n_updn
+
+
+def hubbard_hamiltonian(t=1.0, U=4.0, mu=2.0) -> SchurMPO:
+    """Spinful Hubbard chain via Jordan-Wigner, w = 6, built with ``mpohamiltonian``.
+
+    ``H = -t sum_s (c+_{s,i} c_{s,i+1} + h.c.) + U sum n_up n_dn - mu sum n``.
+    With ``c_{s,i} = (prod_{j<i} P_j) c_s`` the two hopping directions are
+    ``(c+_s P) (x) c_s`` and ``(P c_s) (x) c+_s``, giving four channels.  The
+    reference's own ``fermi_hubbard`` (``src/models.jl:164-178``) has only two
+    channels and a non-Hermitian bond term, so it is not used.
+    """
+    c_up, c_dn, P, n, n_updn = hubbard_operators()
+    h1 = U * n_updn - mu * n
+    pairs = [
+        (-t, c_up.conj().T @ P, c_up),
+        (-t, P @ c_up, c_up.conj().T),
+        (-t, c_dn.conj().T @ P, c_dn),
+        (-t, P @ c_dn, c_dn.conj().T),
+    ]
+    return SchurMPO([mpohamiltonian(h1, pairs)])
+
+
+def tfim_e0(J=1.0, h=1.0) -> float:
+    """Exact TFIM ground-state energy density ``-(1/pi) int_0^pi sqrt(J^2+h^2-2Jh cos k) dk``."""
+    from scipy.integrate import quad
+    v, _ = quad(lambda k: math.sqrt(J * J + h * h - 2 * J * h * math.cos(k)), 0, math.pi, limit=200)
+    return -v / math.pi
+
+
+def hubbard_e0(t=1.0, U=4.0, mu=2.0) -> float:
+    """Lieb-Wu half-filling energy per site minus ``mu * <n>`` (``<n> = 1``)."""
+    from scipy.integrate import quad
+    from scipy.special import j0, j1
+
+    def f(w):
+        x = w * U / (2 * t)
+        if x > 700:
+            return 0.0
+        return j0(w) * j1(w) / (w * (1.0 + math.exp(x)))
+
+    v, _ = quad(f, 0, np.inf, limit=500)
+    return -4 * t * v - mu
+
+
+# --------------------------------------------------------------------------
+# QRpos / LQpos  (FiniteMPSAlgorithms leftorth/rightorth with QRpos/LQpos;
+# usage: src/states/ortho.jl:150-153, 188-191, 214-227)
+# --------------------------------------------------------------------------
+def qrpos(M: np.ndarray):
+    """``leftorth(M; alg = QRpos())``: ``M = Q R`` with a non-negative real diagonal of R."""
+    Q, R = np.linalg.qr(M, mode="reduced")
+    dg = np.diag(R)
+    mag = np.abs(dg)
+    ph = np.where(mag > 0, dg / np.where(mag > 0, mag, 1), 1.0)
+    Q = Q * ph[None, :]
+    R = R * np.conj(ph)[:, None]
+    return np.asfortranarray(Q), np.asfortranarray(R)
+
+
+def lqpos(M: np.ndarray):
+    """``rightorth(M; alg = LQpos())``: ``M = L Q`` with a non-negative real diagonal of L."""
+    Qp, Rp = qrpos(M.conj().T)
+    return np.asfortranarray(Rp.conj().T), np.asfortranarray(Qp.conj().T)
+
+
+# --------------------------------------------------------------------------
+# Krylov solvers (KrylovKit restated; see the module docstring)
+# --------------------------------------------------------------------------
+@dataclass
+class KrylovInfo:
+    converged: int = 0
+    numiter: int = 0
+    numops: int = 0
+    normres: float = float("nan")
+
+
+def _cgs2(V: List[np.ndarray], w: np.ndarray):
+    """Classical Gram-Schmidt with one re-orthogonalisation pass (CGS2)."""
+    if not V:
+        return w, np.zeros(0, dtype=C128)
+    B = np.stack(V, axis=1)
+    h = B.conj().T @ w
+    w = w - B @ h
+    h2 = B.conj().T @ w
+    w = w - B @ h2
+    return w, h + h2
+
+
+def _phase_align(v: np.ndarray, x0: np.ndarray) -> np.ndarray:
+    """Fix the eigenvector phase so that ``<x0, v>`` is real and non-negative."""
+    ov = np.vdot(x0, v)
+    if abs(ov) > 0:
+        v = v * (np.conj(ov) / abs(ov))
+    return v
+
+
+def lanczos_eigsolve(A: Callable, x0: np.ndarray, tol: float, krylovdim: int = 30,
+                     maxiter: int = 300, eager: bool = True, which: str = "SR"):
+    """Smallest-real eigenpair of a Hermitian map (``fixedpoint(.., :SR, Lanczos)``,
+    ``src/utility.jl:180-186``, ``_eigsolve`` ``:379-393``).
+
+    Thick-restart Lanczos with full CGS2 re-orthogonalisation.  The projected
+    matrix is the Hermitian part of the Gram-Schmidt coefficients; a Ritz pair
+    is converged when ``|beta_m u_m| <= tol``.  At a restart the
+    ``keep = (3 krylovdim + 2 converged) // 5`` best Ritz vectors are kept
+    (KrylovKit's shrink rule).  ``maxiter`` counts restart cycles.  The
+    returned vector is normalised and phase-aligned with ``x0``.
+    """
+    shape = x0.shape
+    x0f = np.asarray(x0, dtype=C128).ravel(order="F")
+    n = x0f.size
+    kdim = min(krylovdim, n)
+    beta0 = np.linalg.norm(x0f)
+    if beta0 == 0:
+        raise ValueError("eigsolve: zero starting vector")
+    x0n = x0f / beta0
+    V = [x0n.copy()]
+    H = np.zeros((kdim + 1, kdim), dtype=C128)
+    info = KrylovInfo(numiter=1)
+    sign = 1.0 if which == "SR" else -1.0
+    while True:
+        k = len(V) - 1  # index of the vector to expand
+        w = A(freshape(V[k], shape)).ravel(order="F").astype(C128, copy=False)
+        info.numops += 1
+        w, h = _cgs2(V, w)
+        beta = np.linalg.norm(w)
+        H[: k + 1, k] = h
+        H[k + 1, k] = beta
+        m = k + 1
+        Hs = H[:m, :m]
+        Hs = 0.5 * (Hs + Hs.conj().T)
+        theta, U = np.linalg.eigh(Hs)
+        order = np.argsort(sign * theta, kind="stable")
+        theta, U = theta[order], U[:, order]
+        res = np.abs(beta * U[m - 1, :])
+        breakdown = beta <= 1e-14 * max(1.0, abs(theta).max())
+        full = m == kdim
+        if eager or full or breakdown:
+            if res[0] <= tol or breakdown:
+                info.converged = 1
+                info.normres = float(res[0])
+                vec = np.stack(V, axis=1) @ U[:, 0]
+                vec /= np.linalg.norm(vec)
+                vec = _phase_align(vec, x0n)
+                return float(theta[0]), freshape(vec, shape), info
+        if full:
+            if info.numiter >= maxiter:
+                info.normres = float(res[0])
+                vec = np.stack(V, axis=1) @ U[:, 0]
+                vec /= np.linalg.norm(vec)
+                return float(theta[0]), freshape(vec, shape), info
+            nconv = int(np.sum(res <= tol))
+            keep = max(1, (3 * kdim + 2 * nconv) // 5)
+            B = np.stack(V, axis=1)
+            Vk = B @ U[:, :keep]
+            vnext = w / beta
+            V = [Vk[:, j].copy() for j in range(keep)] + [vnext]
+            H = np.zeros((kdim + 1, kdim), dtype=C128)
+            H[:keep, :keep] = np.diag(theta[:keep])
+            H[keep, :keep] = beta * U[m - 1, :keep]
+            info.numiter += 1
+        else:
+            V.append(w / beta)
+
+
+def gmres(A: Callable, b: np.ndarray, x0: np.ndarray, tol: float, krylovdim: int = 30,
+          maxiter: int = 300, a0: complex = 1.0, a1: complex = 1.0):
+    """``linsolve(op, b, x0, GMRES; a0, a1)`` solving ``(a0 + a1 A) x = b``
+    (``src/algorithms/groundstates/envs.jl:14-19``).
+
+    Restarted GMRES(krylovdim) with CGS2 and Givens rotations; ``tol`` bounds
+    the 2-norm of the residual; ``maxiter`` counts restart cycles.  The true
+    residual is recomputed after every cycle.
+    """
+    shape = b.shape
+    bf = np.asarray(b, dtype=C128).ravel(order="F")
+    x = np.asarray(x0, dtype=C128).ravel(order="F").copy()
+    info = KrylovInfo()
+
+    def op(v):
+        info.numops += 1
+        return a0 * v + a1 * A(freshape(v, shape)).ravel(order="F")
+
+    r = bf - op(x)
+    beta = np.linalg.norm(r)
+    info.normres = float(beta)
+    if beta <= tol:
+        info.converged = 1
+        return freshape(x, shape), info
+    n = bf.size
+    kdim = min(krylovdim, n)
+    while True:
+        info.numiter += 1
+        V = [r / beta]
+        R = np.zeros((kdim + 1, kdim), dtype=C128)
+        cs = np.zeros(kdim, dtype=np.float64)
+        sn = np.zeros(kdim, dtype=C128)
+        g = np.zeros(kdim + 1, dtype=C128)
+        g[0] = beta
+        kused = 0
+        for k in range(kdim):
+            w = op(V[k])
+            w, h = _cgs2(V, w)
+            hn = np.linalg.norm(w)
+            col = np.zeros(k + 2, dtype=C128)
+            col[: k + 1] = h
+            col[k + 1] = hn
+            for j in range(k):
+                t1 = cs[j] * col[j] + sn[j] * col[j + 1]
+                col[j + 1] = -np.conj(sn[j]) * col[j] + cs[j] * col[j + 1]
+                col[j] = t1
+            a, bb = col[k], col[k + 1]
+            nrm = math.hypot(abs(a), abs(bb))
+            if nrm == 0:
+                cs[k], sn[k] = 1.0, 0.0
+            elif abs(a) == 0:
+                cs[k], sn[k] = 0.0, np.conj(bb) / abs(bb)
+                cs[k] = 0.0
+            else:
+                cs[k] = abs(a) / nrm
+                sn[k] = (a / abs(a)) * np.conj(bb) / nrm
+            col[k] = cs[k] * a + sn[k] * bb
+            col[k + 1] = 0.0
+            g[k + 1] = -np.conj(sn[k]) * g[k]
+            g[k] = cs[k] * g[k]
+            R[: k + 2, k] = col
+            kused = k + 1
+            if abs(g[k + 1]) <= tol or hn <= 1e-300:
+                break
+            V.append(w / hn)
+        # back substitution
+        y = np.zeros(kused, dtype=C128)
+        for i in range(kused - 1, -1, -1):
+            y[i] = (g[i] - R[i, i + 1:kused] @ y[i + 1:kused]) / R[i, i]
+        x = x + np.stack(V[:kused], axis=1) @ y
+        r = bf - op(x)
+        beta = np.linalg.norm(r)
+        info.normres = float(beta)
+        if beta <= tol:
+            info.converged = 1
+            return freshape(x, shape), info
+        if info.numiter >= maxiter:
+            return freshape(x, shape), info
+
+
+def _expm_herm(Hs: np.ndarray, t: complex) -> np.ndarray:
+    th, U = np.linalg.eigh(Hs)
+    return (U * np.exp(t * th)[None, :]) @ U.conj().T
+
+
+def exponentiate(A: Callable, t: complex, x: np.ndarray, tol: float = 1e-10,
+                 krylovdim: int = 30, maxiter: int = 300):
+    """``exponentiate(A, t, x; ishermitian = true)`` (``src/algorithms/timeevo/tdvp.jl:14-20``).
+
+    Lanczos (full CGS2) Krylov exponential with time sub-stepping.  For a
+    remaining step ``tau`` the a-posteriori error estimate of the basis of size
+    ``m`` is ``beta |h_{m+1,m}| |[exp(tau H_m) e1]_m|``; a step is accepted when
+    the estimate is at most ``tol |tau| / |t|``.  When the basis is full and the
+    whole remainder is not accepted, ``tau`` is halved until it is.  ``maxiter``
+    bounds the number of accepted sub-steps.
+    """
+    shape = x.shape
+    v = np.asarray(x, dtype=C128).ravel(order="F").copy()
+    info = KrylovInfo()
+    T = complex(t)
+    if T == 0:
+        info.converged = 1
+        return freshape(v, shape), info
+    remaining = T
+    n = v.size
+    kdim = min(krylovdim, n)
+    while True:
+        beta = np.linalg.norm(v)
+        if beta == 0:
+            info.converged = 1
+            return freshape(v, shape), info
+        info.numiter += 1
+        V = [v / beta]
+        H = np.zeros((kdim + 1, kdim), dtype=C128)
+        tau = remaining
+        accepted = False
+        while True:
+            k = len(V) - 1
+            w = A(freshape(V[k], shape)).ravel(order="F").astype(C128, copy=False)
+            info.numops += 1
+            w, h = _cgs2(V, w)
+            hn = np.linalg.norm(w)
+            H[: k + 1, k] = h
+            H[k + 1, k] = hn
+            m = k + 1
+            Hs = H[:m, :m]
+            Hs = 0.5 * (Hs + Hs.conj().T)
+            breakdown = hn <= 1e-14 * max(1.0, np.abs(np.diag(Hs)).max())
+            E = _expm_herm(Hs, tau)
+            err = beta * hn * abs(E[m - 1, 0])
+            if breakdown or err <= tol * abs(tau) / abs(T):
+                accepted = True
+                break
+            if m == kdim:
+                while err > tol * abs(tau) / abs(T) and abs(tau) > 1e-300:
+                    tau = tau / 2
+                    E = _expm_herm(Hs, tau)
+                    err = beta * hn * abs(E[m - 1, 0])
+                accepted = True
+                break
+            V.append(w / hn)
+        if accepted:
+            m = len(V)
+            E = _expm_herm(Hs, tau)
+            v = beta * (np.stack(V, axis=1) @ E[:, 0])
+            remaining = remaining - tau
+            info.normres = float(err)
+            if abs(remaining) <= 1e-15 * abs(T):
+                info.converged = 1
+                return freshape(v, shape), info
+            if info.numiter >= maxiter:
+                return freshape(v, shape), info
+
+
+def arnoldi_dominant(A: Callable, x0: np.ndarray, tol: float, krylovdim: int = 30,
+                     maxiter: int = 300, eager: bool = True):
+    """Dominant (largest-magnitude) eigenpair of a non-Hermitian map.
+
+    Restates ``gauge_fixedpoint`` (KrylovKit ``schursolve``, ``src/utility.jl:204-211``)
+    and the ``:LM`` Arnoldi of ``dot(psi, psi)`` (``src/states/canonicalmps.jl:262-269``).
+    Arnoldi with CGS2; a Ritz pair is converged when ``|h_{m+1,m} y_m| <= tol``
+    (``y`` normalised).  A full basis restarts from the current dominant Ritz
+    vector.  The vector is normalised and phase-aligned with ``x0``.
+    """
+    shape = x0.shape
+    x0f = np.asarray(x0, dtype=C128).ravel(order="F")
+    n = x0f.size
+    kdim = min(krylovdim, n)
+    x0n = x0f / np.linalg.norm(x0f)
+    V = [x0n.copy()]
+    H = np.zeros((kdim + 1, kdim), dtype=C128)
+    info = KrylovInfo(numiter=1)
+    while True:
+        k = len(V) - 1
+        w = A(freshape(V[k], shape)).ravel(order="F").astype(C128, copy=False)
+        info.numops += 1
+        w, h = _cgs2(V, w)
+        hn = np.linalg.norm(w)
+        H[: k + 1, k] = h
+        H[k + 1, k] = hn
+        m = k + 1
+        lam, Y = np.linalg.eig(H[:m, :m])
+        j = int(np.argmax(np.abs(lam)))
+        y = Y[:, j] / np.linalg.norm(Y[:, j])
+        res = abs(hn * y[m - 1])
+        breakdown = hn <= 1e-14 * max(1.0, abs(lam[j]))
+        full = m == kdim
+        if eager or full or breakdown:
+            if res <= tol or breakdown:
+                info.converged = 1
+                info.normres = float(res)
+                vec = np.stack(V, axis=1) @ y
+                vec /= np.linalg.norm(vec)
+                return complex(lam[j]), freshape(_phase_align(vec, x0n), shape), info
+        if full:
+            vec = np.stack(V, axis=1) @ y
+            vec /= np.linalg.norm(vec)
+            if info.numiter >= maxiter:
+                info.normres = float(res)
+                return complex(lam[j]), freshape(vec, shape), info
+            V = [vec]
+            H = np.zeros((kdim + 1, kdim), dtype=C128)
+            info.numiter += 1
+        else:
+            V.append(w / hn)
+
+
+# --------------------------------------------------------------------------
+# Transfer pushes  (src/transfermatrix.jl:5-66, src/algorithms/groundstates/envs.jl:104-114, 199-231)
+# --------------------------------------------------------------------------
+def push_env_left(L, above, below=None):
+    """``L'[a',b'] = sum conj(below[a,s,a']) L[a,b] above[b,s,b']`` (``transfermatrix.jl:5-7, 54-58``)."""
+    below = above if below is None else below
+    Dl, d, Dr = above.shape
+    Y = L @ freshape(above, (Dl, d * Dr))
+    return np.asfortranarray(freshape(below, (below.shape[0] * d, below.shape[2])).conj().T @ freshape(Y, (Dl * d, Dr)))
+
+
+def push_env_right(R, above, below=None):
+    """``R'[a',b'] = sum above[a',s,a] R[a,b] conj(below[b',s,b])`` (``transfermatrix.jl:23-26, 62-66``)."""
+    below = above if below is None else below
+    Dl, d, Dr = above.shape
+    Y = freshape(above, (Dl * d, Dr)) @ R
+    return np.asfortranarray(freshape(Y, (Dl, d * R.shape[1])) @ freshape(below, (below.shape[0], d * below.shape[2])).conj().T)
+
+
+def push_slice_left(L, Wl, A):
+    """``_push_slice_left`` (``envs.jl:104-107``): ``sum conj(A[a,u,a']) L[a,b] Wl[u,d] A[b,d,b']``."""
+    Dl, d, Dr = A.shape
+    Y = freshape(L @ freshape(A, (Dl, d * Dr)), (Dl, d, Dr))
+    Z = np.einsum("ud,adb->aub", Wl, Y)
+    return np.asfortranarray(freshape(A, (Dl * d, Dr)).conj().T @ freshape(np.asfortranarray(Z), (Dl * d, Dr)))
+
+
+def push_slice_right(R, Wl, A):
+    """``_push_slice_right`` (``envs.jl:111-114``): ``sum A[a',d,a] R[a,b] Wl[u,d] conj(A[b',u,b])``."""
+    Dl, d, Dr = A.shape
+    Y = freshape(freshape(A, (Dl * d, Dr)) @ R, (Dl, d, Dr))
+    Z = np.einsum("ud,adb->aub", Wl, Y)
+    return np.asfortranarray(freshape(np.asfortranarray(Z), (Dl, d * Dr)) @ freshape(A, (Dl, d * Dr)).conj().T)
+
+
+def push_mpo_left(L, W, A):
+    """Schur/dense MPO left push (``envs.jl:199-210``, ``transfermatrix.jl:11-13``):
+    ``L'[a',j,b'] = sum conj(A[a,u,a']) L[a,i,b] W[i,u,j,d] A[b,d,b']``."""
+    Dl, d, Dr = A.shape
+    m, n = W.shape[0], W.shape[2]
+    Y = freshape(freshape(L, (Dl * m, Dl)) @ freshape(A, (Dl, d * Dr)), (Dl, m, d, Dr))
+    Z = np.einsum("iujd,aidb->aujb", W, Y)
+    out = freshape(A, (Dl * d, Dr)).conj().T @ freshape(np.asfortranarray(Z), (Dl * d, n * Dr))
+    return np.asfortranarray(freshape(out, (Dr, n, Dr)))
+
+
+def push_mpo_right(R, W, A):
+    """Schur/dense MPO right push (``envs.jl:220-231``, ``transfermatrix.jl:31-35``):
+    ``R'[a',i,b'] = sum A[a',d,a] W[i,u,j,d] conj(A[b',u,b]) R[a,j,b]``."""
+    Dl, d, Dr = A.shape
+    m, n = W.shape[0], W.shape[2]
+    Y = freshape(freshape(A, (Dl * d, Dr)) @ freshape(R, (Dr, n * Dr)), (Dl, d, n, Dr))
+    Z = np.einsum("iujd,adjb->aiub", W, Y)
+    out = freshape(np.asfortranarray(Z), (Dl * m, d * Dr)) @ freshape(A, (Dl, d * Dr)).conj().T
+    return np.asfortranarray(freshape(out, (Dl, m, Dl)))
+
+
+def regularize(v, lvec, rvec):
+    """``regularize!(v, lvec, rvec)`` (``envs.jl:28-32``): ``v - tr(lvec v) rvec`` (no conjugation)."""
+    c = np.sum(lvec * v.T)
+    return np.asfortranarray(v - c * rvec)
+
+
+# --------------------------------------------------------------------------
+# States: CanonicalIMPS and gauge fixing  (src/states/canonicalmps.jl, ortho.jl)
+# --------------------------------------------------------------------------
+@dataclass
+class CanonicalIMPS:
+    """``CanonicalIMPS`` (``canonicalmps.jl:17-40``): ``AL[i] C[i] = AC[i] = C[i-1] AR[i]``."""
+    AL: List[np.ndarray]
+    AR: List[np.ndarray]
+    C: List[np.ndarray]
+    AC: List[np.ndarray]
+
+    def __len__(self):
+        return len(self.AL)
+
+    def copy(self):
+        return CanonicalIMPS([a.copy(order="F") for a in self.AL], [a.copy(order="F") for a in self.AR],
+                             [c.copy(order="F") for c in self.C], [a.copy(order="F") for a in self.AC])
+
+    def Cm(self, l):
+        """Periodic access to ``C[l]`` with Julia's 1-based site labels (``C[0] = C[N]``)."""
+        return self.C[(l - 1) % len(self.C)]
+
+
+def _mulAL(AL, C):
+    Dl, d, Dr = AL.shape
+    return np.asfortranarray(freshape(freshape(AL, (Dl * d, Dr)) @ C, (Dl, d, C.shape[1])))
+
+
+def _mulCA(C, A):
+    Dl, d, Dr = A.shape
+    return np.asfortranarray(freshape(C @ freshape(A, (Dl, d * Dr)), (C.shape[0], d, Dr)))
+
+
+def _fnorm(x):
+    return float(np.linalg.norm(np.asarray(x).ravel()))
+
+
+def _gauge_eig_tol(eps):
+    # _GAUGE_ALG_EIGSOLVE = alg_eigsolve(ishermitian=false, tol_factor=1)  (ortho.jl:6)
+    return min(max(eps ** 2, Defaults.tol_min), Defaults.tol_max)
+
+
+def uniform_leftorth(A: List[np.ndarray], C0: np.ndarray, tol=Defaults.tolgauge,
+                     maxiter=Defaults.maxiter, eig_miniter=10):
+    """``uniform_leftorth!`` (``ortho.jl:125-164``). Returns ``(AL, C, info)``,
+    ``C[i]`` the bond matrix right of site ``i`` (0-based list, ``C[-1] = C[N]``)."""
+    N = len(A)
+    Awork = [a.copy(order="F") for a in A]
+    C = [None] * N
+    C[N - 1] = C0 / _fnorm(C0)
+    AL = [None] * N
+    it = 0
+    eps = math.inf
+    while True:
+        if it >= eig_miniter:
+            etol = _gauge_eig_tol(eps)
+
+            def tm(v):
+                L = v
+                for l in range(N):
+                    L = push_env_left(L, Awork[l], AL[l])
+                return L
+            _, evec, _ = arnoldi_dominant(tm, C[N - 1], etol)
+            _, C[N - 1] = qrpos(evec)
+        Cpre = C[N - 1].copy()
+        for i in range(N):
+            Dl_, d, Dr_ = Awork[i].shape
+            M = _mulCA(C[i - 1], Awork[i])
+            Q, Rf = qrpos(freshape(M, (M.shape[0] * d, Dr_)))
+            AL[i] = np.asfortranarray(freshape(Q, (M.shape[0], d, Q.shape[1])))
+            C[i] = Rf
+        C[N - 1] = C[N - 1] / _fnorm(C[N - 1])
+        eps = _fnorm(C[N - 1] - Cpre)
+        it += 1
+        if eps < tol or it > maxiter:
+            return AL, C, dict(niter=it, err=eps, converged=eps < tol)
+
+
+def uniform_rightorth(A: List[np.ndarray], C0: np.ndarray, tol=Defaults.tolgauge,
+                      maxiter=Defaults.maxiter, eig_miniter=10):
+    """``uniform_rightorth!`` (``ortho.jl:166-202``). Returns ``(AR, C, info)``."""
+    N = len(A)
+    Awork = [a.copy(order="F") for a in A]
+    C = [None] * N
+    C[N - 1] = C0 / _fnorm(C0)
+    AR = [None] * N
+    it = 0
+    eps = math.inf
+    while True:
+        if it >= eig_miniter:
+            etol = _gauge_eig_tol(eps)
+
+            def tm(v):
+                R = v
+                for l in range(N - 1, -1, -1):
+                    R = push_env_right(R, Awork[l], AR[l])
+                return R
+            _, evec, _ = arnoldi_dominant(tm, C[N - 1], etol)
+            C[N - 1], _ = lqpos(evec)
+        Cpre = C[N - 1].copy()
+        for i in range(N - 1, -1, -1):
+            Dl_, d, Dr_ = Awork[i].shape
+            M = _mulAL(Awork[i], C[i])
+            Lf, Q = lqpos(freshape(M, (Dl_, d * M.shape[2])))
+            AR[i] = np.asfortranarray(freshape(Q, (Lf.shape[1], d, M.shape[2])))
+            C[i - 1] = Lf
+        C[N - 1] = C[N - 1] / _fnorm(C[N - 1])
+        eps = _fnorm(C[N - 1] - Cpre)
+        it += 1
+        if eps < tol or it > maxiter:
+            return AR, C, dict(niter=it, err=eps, converged=eps < tol)
+
+
+def gaugefix(A: List[np.ndarray], C0: np.ndarray, order="LR", tol=Defaults.tolgauge,
+             maxiter=Defaults.maxiter, AL_given=None) -> CanonicalIMPS:
+    """``gaugefix!`` (``ortho.jl:64-99``) returning a fresh ``CanonicalIMPS``.
+
+    ``order='LR'``: left-orthogonalise ``A`` from ``C0``, then right-orthogonalise
+    the resulting ``AL`` from ``C[N]``; ``AC = AL C``.  ``order='R'``: ``AL`` is
+    kept as given (``A``), ``AR, C`` come from ``uniform_rightorth!``; ``AC = C AR``.
+    """
+    N = len(A)
+    if order == "LR":
+        AL, C, _ = uniform_leftorth(A, C0, tol, maxiter)
+        AR, C, _ = uniform_rightorth(AL, C[N - 1], tol, maxiter)
+        AC = [_mulCA(C[i - 1], AR[i]) for i in range(N)]
+        return CanonicalIMPS(AL, AR, C, AC)
+    if order == "R":
+        AL = [a.copy(order="F") for a in A]
+        AR, C, _ = uniform_rightorth(A, C0, tol, maxiter)
+        AC = [_mulCA(C[i - 1], AR[i]) for i in range(N)]
+        return CanonicalIMPS(AL, AR, C, AC)
+    raise ValueError(f"invalid order {order}")
+
+
+def canonical_from_AL(ALs: List[np.ndarray], C0: np.ndarray, tol=Defaults.tolgauge,
+                      maxiter=Defaults.maxiter) -> CanonicalIMPS:
+    """``CanonicalIMPS(ALs, C0)`` (``canonicalmps.jl:180-195``): right gauge fix, ``AC = AL C``."""
+    psi = gaugefix(ALs, C0, order="R", tol=tol, maxiter=maxiter)
+    psi.AC = [_mulAL(psi.AL[i], psi.C[i]) for i in range(len(ALs))]
+    return psi
+
+
+def canonical_from_sites(As: List[np.ndarray], tol=Defaults.tolgauge, maxiter=Defaults.maxiter):
+    """``CanonicalIMPS(As)`` (``canonicalmps.jl:151-170``) for full-rank uniform-bond input:
+    ``gaugefix!(:LR)`` from ``C0 = I`` then ``AC = AL C``."""
+    D = As[0].shape[0]
+    psi = gaugefix(As, np.eye(D, dtype=C128, order="F"), order="LR", tol=tol, maxiter=maxiter)
+    psi.AC = [_mulAL(psi.AL[i], psi.C[i]) for i in range(len(As))]
+    return psi
+
+
+def random_site_tensors(dims: Sequence[int], D: int, seed: int) -> List[np.ndarray]:
+    """Seeded i.i.d. complex-normal site tensors (Re, Im ~ N(0, 1/2)), NumPy PCG64.
+
+    Stands in for Julia's ``randn(rng, ComplexF64, D, d, D)`` (``constructors.jl:13-22``);
+    the same arrays are fed to the oracle and to the GPU.
+    """
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for d in dims:
+        re = rng.standard_normal((D, d, D))
+        im = rng.standard_normal((D, d, D))
+        out.append(np.asfortranarray((re + 1j * im) / math.sqrt(2.0)))
+    return out
+
+
+def randomimps(dims: Sequence[int], D: int, seed: int, **kw) -> CanonicalIMPS:
+    """``randomimps(ComplexF64, dims; D)`` (``constructors.jl:13-22``) with a PCG64 seed."""
+    return canonical_from_sites(random_site_tensors(dims, D, seed), **kw)
+
+
+def regauge(AC: np.ndarray, C: np.ndarray) -> np.ndarray:
+    """``regauge!(AC, C)`` (``ortho.jl:214-219``): ``AL = Q(AC) Q(C)^H`` with QRpos."""
+    Dl, d, Dr = AC.shape
+    Qac, _ = qrpos(freshape(AC, (Dl * d, Dr)))
+    Qc, _ = qrpos(C)
+    return np.asfortranarray(freshape(Qac @ Qc.conj().T, (Dl, d, Dr)))
+
+
+def state_dot(psi1: CanonicalIMPS, psi2: CanonicalIMPS, krylovdim=Defaults.krylovdim) -> complex:
+    """``dot(psi1, psi2)`` (``canonicalmps.jl:262-269``): dominant eigenvalue of
+    ``TransferMatrix(psi2.AL, psi1.AL)`` from ``v0 = I`` (Arnoldi, ``tol = 1e-10``)."""
+    N = len(psi1)
+    D0 = psi1.AL[0].shape[0]
+    v0 = np.eye(D0, psi2.AL[0].shape[0], dtype=C128, order="F")
+
+    def tm(v):
+        L = v
+        for l in range(N):
+            L = push_env_left(L, psi2.AL[l], psi1.AL[l])
+        return L
+    lam, _, _ = arnoldi_dominant(tm, v0, Defaults.tol, krylovdim)
+    return lam
+
+
+# --------------------------------------------------------------------------
+# Environments: DMRGCache(psi, ::SparseIMPO)  (src/algorithms/groundstates/envs.jl:121-188, 321-546)
+# --------------------------------------------------------------------------
+@dataclass
+class DMRGCache:
+    """Schur-Hamiltonian environments: ``lefts[l]`` is ``(chi_{l-1}, m_l, chi_{l-1})``
+    (bra, level, ket) and ``rights[l]`` is ``(chi_l, n_l, chi_l)`` (ket, level, bra)."""
+    lefts: List[np.ndarray]
+    rights: List[np.ndarray]
+    stats: dict = field(default_factory=dict)
+
+    def leftenv(self, l):
+        return self.lefts[l % len(self.lefts)]
+
+    def rightenv(self, l):
+        return self.rights[l % len(self.rights)]
+
+
+def _left_cyclethrough(lefts, H, AL, i, N):
+    """``_left_cyclethrough!`` (``envs.jl:121-136``); ``i`` is 1-based; zero blocks skipped."""
+    for site in range(N):
+        snext = (site + 1) % N
+        chi = AL[site].shape[2]
+        W = H[site]
+        ms, ns = W.shape[0], W.shape[2]
+        if not (i <= ns - 1):
+            continue
+        tgt = fzeros((chi, chi))
+        for l in range(1, min(i, ms) + 1):
+            blk = W[l - 1, :, i - 1, :]
+            if not np.any(blk):
+                continue
+            tgt += push_slice_left(np.asfortranarray(lefts[site][:, l - 1, :]), blk, AL[site])
+        lefts[snext][:, i - 1, :] = tgt
+
+
+def _left_closing_sweep(lefts, H, AL, N):
+    """``_left_closing_sweep!`` (``envs.jl:143-156``)."""
+    for site in range(N):
+        snext = (site + 1) % N
+        chi = AL[site].shape[2]
+        W = H[site]
+        ms, ns = W.shape[0], W.shape[2]
+        tgt = fzeros((chi, chi))
+        for l in range(1, ms + 1):
+            blk = W[l - 1, :, ns - 1, :]
+            if not np.any(blk):
+                continue
+            tgt += push_slice_left(np.asfortranarray(lefts[site][:, l - 1, :]), blk, AL[site])
+        lefts[snext][:, ns - 1, :] = tgt
+
+
+def _right_cyclethrough(rights, H, AR, i, N):
+    """``_right_cyclethrough!`` (``envs.jl:162-177``)."""
+    for site in range(N - 1, -1, -1):
+        sprev = (site - 1) % N
+        chi = AR[site].shape[0]
+        W = H[site]
+        ms, ns = W.shape[0], W.shape[2]
+        if not (i <= ms):
+            continue
+        tgt = fzeros((chi, chi))
+        for l in range(i, ns + 1):
+            blk = W[i - 1, :, l - 1, :]
+            if not np.any(blk):
+                continue
+            tgt += push_slice_right(np.asfortranarray(rights[site][:, l - 1, :]), blk, AR[site])
+        rights[sprev][:, i - 1, :] = tgt
+
+
+def _diag_channel(W, i):
+    """``_diag_channel`` (``envs.jl:182-188``)."""
+    if i <= min(W.shape[0], W.shape[2]):
+        return W[i - 1, :, i - 1, :]
+    return np.zeros((W.shape[1], W.shape[3]), dtype=C128)
+
+
+def build_envs(psi: CanonicalIMPS, H: SchurMPO, tol=Defaults.tol, maxiter=Defaults.maxiter,
+               krylovdim=Defaults.krylovdim, init: Optional[DMRGCache] = None) -> DMRGCache:
+    """``DMRGCache(psi, H::SparseIMPO; tol, maxiter, krylovdim, init_lefts, init_rights)``
+    (``envs.jl:321-518``), step for step."""
+    N = len(psi)
+    Dl = [psi.AL[l].shape[0] for l in range(N)]
+    Dr = [psi.AL[l].shape[2] for l in range(N)]
+    if H[N - 1].shape[2] != H[0].shape[0]:
+        raise ValueError("operator level chain does not close over the ket unit cell")
+    ml = [H[l].shape[0] for l in range(N)]
+    nr = [H[l].shape[2] for l in range(N)]
+    lefts = [fzeros((Dl[l], ml[l], Dl[l])) for l in range(N)]
+    rights = [fzeros((Dr[l], nr[l], Dr[l])) for l in range(N)]
+    for l in range(N):
+        lefts[l][:, 0, :] = np.eye(Dl[l])
+        rights[l][:, nr[l] - 1, :] = np.eye(Dr[l])
+    kdim = min(Dl[0] * Dl[0], krylovdim)
+    stats = dict(gmres_iters=0, gmres_ops=0, solves=0)
+    AL, AR = psi.AL, psi.AR
+
+    def solve(op, rhs, prev):
+        x, info = gmres(op, rhs, prev, tol, kdim, maxiter, 1.0, -1.0)
+        stats["gmres_iters"] += info.numiter
+        stats["gmres_ops"] += info.numops
+        stats["solves"] += 1
+        return x
+
+    CN = psi.C[N - 1]
+    jmax = max(nr) - 1
+    # ---- left environments (envs.jl:363-421)
+    for i in range(2, jmax + 1):
+        if i <= ml[0] - 1:
+            D = Dl[0]
+            if init is not None and init.lefts[0].shape == lefts[0].shape:
+                prev = np.asfortranarray(init.lefts[0][:, i - 1, :])
+            else:
+                prev = np.asfortranarray(lefts[0][:, i - 1, :])
+            _left_cyclethrough(lefts, H, AL, i, N)
+            rhs = np.asfortranarray(lefts[0][:, i - 1, :])
+            if H.isidentitylevel(i):
+                rho_r = CN @ CN.conj().T
+                I1 = np.eye(D, dtype=C128)
+
+                def op(v):
+                    X = v
+                    for l in range(N):
+                        X = push_env_left(X, AL[l])
+                    return regularize(X, rho_r, I1)
+                lefts[0][:, i - 1, :] = solve(op, rhs, prev)
+                if N > 1:
+                    _left_cyclethrough(lefts, H, AL, i, N)
+                for l in range(N):
+                    Cp = psi.C[l - 1]
+                    lefts[l][:, i - 1, :] = regularize(np.asfortranarray(lefts[l][:, i - 1, :]), Cp @ Cp.conj().T, np.eye(Dl[l]))
+            else:
+                if not H.isemptylevel(i):
+                    def op(v, i=i):
+                        X = v
+                        for l in range(N):
+                            blk = _diag_channel(H[l], i)
+                            X = push_slice_left(X, blk, AL[l]) if np.any(blk) else fzeros((AL[l].shape[2], AL[l].shape[2]))
+                        return X
+                    lefts[0][:, i - 1, :] = solve(op, rhs, prev)
+                if N > 1:
+                    _left_cyclethrough(lefts, H, AL, i, N)
+        else:
+            _left_cyclethrough(lefts, H, AL, i, N)
+    # ---- closing level of the left environments (envs.jl:424-455)
+    i = ml[0]
+    D = Dl[0]
+    if init is not None and init.lefts[0].shape == lefts[0].shape:
+        prev = np.asfortranarray(init.lefts[0][:, i - 1, :])
+    else:
+        prev = np.asfortranarray(lefts[0][:, i - 1, :])
+    _left_closing_sweep(lefts, H, AL, N)
+    rhs = np.asfortranarray(lefts[0][:, i - 1, :])
+    rho_r = CN @ CN.conj().T
+    I1 = np.eye(D, dtype=C128)
+
+    def opL(v):
+        X = v
+        for l in range(N):
+            X = push_env_left(X, AL[l])
+        return regularize(X, rho_r, I1)
+    lefts[0][:, i - 1, :] = solve(opL, rhs, prev)
+    if N > 1:
+        _left_closing_sweep(lefts, H, AL, N)
+    for l in range(N):
+        Cp = psi.C[l - 1]
+        lefts[l][:, ml[l] - 1, :] = regularize(np.asfortranarray(lefts[l][:, ml[l] - 1, :]), Cp @ Cp.conj().T, np.eye(Dl[l]))
+    # ---- right environments (envs.jl:461-515)
+    for i in range(jmax, 0, -1):
+        if i <= nr[N - 1] - 1:
+            D = Dr[N - 1]
+            if init is not None and init.rights[N - 1].shape == rights[N - 1].shape:
+                prev = np.asfortranarray(init.rights[N - 1][:, i - 1, :])
+            else:
+                prev = np.asfortranarray(rights[N - 1][:, i - 1, :])
+            _right_cyclethrough(rights, H, AR, i, N)
+            rhs = np.asfortranarray(rights[N - 1][:, i - 1, :])
+            if H.isidentitylevel(i):
+                rho_l = CN.conj().T @ CN
+                IN = np.eye(D, dtype=C128)
+
+                def op(v):
+                    X = v
+                    for l in range(N - 1, -1, -1):
+                        X = push_env_right(X, AR[l])
+                    return regularize(X, rho_l, IN)
+                rights[N - 1][:, i - 1, :] = solve(op, rhs, prev)
+                if N > 1:
+                    _right_cyclethrough(rights, H, AR, i, N)
+                for l in range(N):
+                    Cl = psi.C[l]
+                    rights[l][:, i - 1, :] = regularize(np.asfortranarray(rights[l][:, i - 1, :]), Cl.conj().T @ Cl, np.eye(Dr[l]))
+            else:
+                if not H.isemptylevel(i):
+                    def op(v, i=i):
+                        X = v
+                        for l in range(N - 1, -1, -1):
+                            blk = _diag_channel(H[l], i)
+                            X = push_slice_right(X, blk, AR[l]) if np.any(blk) else fzeros((AR[l].shape[0], AR[l].shape[0]))
+                        return X
+                    rights[N - 1][:, i - 1, :] = solve(op, rhs, prev)
+                if N > 1:
+                    _right_cyclethrough(rights, H, AR, i, N)
+        else:
+            _right_cyclethrough(rights, H, AR, i, N)
+    return DMRGCache(lefts, rights, stats)
+
+
+# --------------------------------------------------------------------------
+# Effective Hamiltonians  (src/algorithms/groundstates/effective.jl:72-102)
+# --------------------------------------------------------------------------
+def ac_apply(GL, W, GR, x):
+    """``MPO_AC_Hamiltonian`` action (``effective.jl:79-102``):
+    ``y[b,u,c] = sum GL[b,i,a] x[a,s,bb] W[i,u,j,s] GR[bb,j,c]`` (linear, no conj).
+
+    Contraction order: ``GL x`` (one GEMM over all left levels), the W mixing,
+    then one GEMM with ``GR`` over all right levels.
+    """
+    Dl, d, Dr = x.shape
+    m, n = W.shape[0], W.shape[2]
+    T1 = freshape(freshape(GL, (Dl * m, Dl)) @ freshape(x, (Dl, d * Dr)), (Dl, m, d, Dr))
+    T2 = np.asfortranarray(np.einsum("iujs,bisc->bucj", W, T1))
+    y = freshape(T2, (Dl * d, Dr * n)) @ freshape(GR, (Dr * n, GR.shape[2]))
+    return np.asfortranarray(freshape(y, (Dl, d, GR.shape[2])))
+
+
+def c_apply(GL, GR, x):
+    """``MPO_C_Hamiltonian`` action (``effective.jl:72-76``):
+    ``y[a,b] = sum GL[a,w,a'] x[a',b'] GR[b',w,b]``."""
+    D1, w, _ = GL.shape
+    D2 = x.shape[1]
+    T = freshape(freshape(GL, (D1 * w, D1)) @ x, (D1, w, D2))
+    T = np.asfortranarray(T.transpose(0, 2, 1))  # [a, b', w]
+    y = freshape(T, (D1, D2 * w)) @ freshape(GR, (D2 * w, GR.shape[2]))
+    return np.asfortranarray(y)
+
+
+def calc_galerkin(psi: CanonicalIMPS, H: SchurMPO, envs: DMRGCache) -> float:
+    """``calc_galerkin`` (``src/algorithms/groundstates/vumps.jl:111-124``)."""
+    eps = 0.0
+    for site in range(len(psi)):
+        x = ac_apply(envs.lefts[site], H[site], envs.rights[site], psi.AC[site])
+        x = x / _fnorm(x)
+        AL = psi.AL[site]
+        Dl, d, Dr = AL.shape
+        A2 = freshape(AL, (Dl * d, Dr))
+        x2 = freshape(x, (Dl * d, Dr))
+        q = A2.conj().T @ x2
+        eps = max(eps, _fnorm(x2 - A2 @ q))
+    return eps
+
+
+def expectationvalue(psi: CanonicalIMPS, H: SchurMPO, envs: DMRGCache) -> complex:
+    """Schur energy (``src/observables/expval.jl:93-112``): per site the closing column
+    ``sum_l <AC| GL_l W[l, n] GR_n |AC>``, divided by ``dot(psi, psi)``."""
+    E = 0.0j
+    for site in range(len(psi)):
+        W = H[site]
+        ms, ns = W.shape[0], W.shape[2]
+        Wcol = fzeros((ms, W.shape[1], 1, W.shape[3]))
+        Wcol[:, :, 0, :] = W[:, :, ns - 1, :]
+        GR = envs.rights[site]
+        GRe = np.asfortranarray(GR[:, ns - 1:ns, :])
+        y = ac_apply(envs.lefts[site], Wcol, GRe, psi.AC[site])
+        E += np.vdot(psi.AC[site], y)
+    return E / state_dot(psi, psi)
+
+
+def local_expectation1(psi: CanonicalIMPS, site: int, O: np.ndarray) -> complex:
+    """``_local_expectation1`` (``expval.jl:33-37``)."""
+    AC = psi.AC[site]
+    E = np.einsum("aub,us,asb->", AC.conj(), O, AC)
+    return E / state_dot(psi, psi)
+
+
+# --------------------------------------------------------------------------
+# Algorithms  (vumps.jl, tdvp.jl, idmrg.jl, algdefs.jl)
+# --------------------------------------------------------------------------
+@dataclass
+class VUMPS:
+    """``VUMPS`` (``src/algorithms/algdefs.jl:26-35``)."""
+    D: int = Defaults.D
+    tol: float = Defaults.tol
+    maxiter: int = Defaults.maxiter
+    verbosity: int = Defaults.verbosity
+    alg_gauge: object = field(default_factory=alg_gauge)
+    alg_eigsolve: object = field(default_factory=alg_eigsolve)
+    alg_environments: object = field(default_factory=alg_environments)
+    finalize: Optional[Callable] = None
+
+
+@dataclass
+class IDMRG:
+    """``IDMRG`` (``src/algorithms/algdefs.jl:72-82``)."""
+    D: int = Defaults.D
+    tol: float = Defaults.tol
+    maxiter: int = Defaults.maxiter
+    verbosity: int = Defaults.verbosity
+    alg_gauge: object = field(default_factory=alg_gauge)
+    alg_environments: object = field(default_factory=alg_environments)
+    alg_eigsolve: object = field(default_factory=alg_eigsolve)
+    finalize: Optional[Callable] = None
+
+
+@dataclass
+class TDVP:
+    """``TDVP`` (``src/algorithms/algdefs.jl:167-173``)."""
+    integrator: dict = field(default_factory=alg_expsolve)
+    alg_gauge: object = field(default_factory=alg_gauge)
+    verbosity: int = Defaults.verbosity
+    finalize: Optional[Callable] = None
+
+
+def _eig_params(alg):
+    a = alg.alg if isinstance(alg, DynamicTol) else alg
+    return a
+
+
+def find_groundstate(psi0: CanonicalIMPS, H: SchurMPO, alg: VUMPS, envs: Optional[DMRGCache] = None,
+                     log: Optional[list] = None):
+    """``find_groundstate(psi0, H, ::VUMPS)`` (``src/algorithms/groundstates/vumps.jl:285-320``).
+
+    Returns ``(psi, envs, info)`` with ``info = dict(niter, converged, losses, itererr)``.
+    """
+    psi = psi0.copy()
+    if envs is None:
+        envs = build_envs(psi, H)
+    eps = calc_galerkin(psi, H, envs)
+    ae = updatetol(alg.alg_environments, 0, eps)
+    envs = build_envs(psi, H, tol=ae["tol"], maxiter=ae["maxiter"], init=envs)
+    losses = [eps]
+    converged = False
+    it = 0
+    N = len(psi)
+    for it in range(1, alg.maxiter + 1):
+        siter = it - 1
+        ea = updatetol(alg.alg_eigsolve, siter, eps)
+        ALs = []
+        for site in range(N):
+            GL, W, GR = envs.lefts[site], H[site], envs.rights[site]
+            _, AC, _ = lanczos_eigsolve(lambda x: ac_apply(GL, W, GR, x), psi.AC[site], ea["tol"],
+                                        ea["krylovdim"], ea["maxiter"], ea["eager"])
+            GLc = envs.lefts[(site + 1) % N]
+            _, C, _ = lanczos_eigsolve(lambda x: c_apply(GLc, GR, x), psi.C[site], ea["tol"],
+                                       ea["krylovdim"], ea["maxiter"], ea["eager"])
+            ALs.append(regauge(AC, C))
+        ag = updatetol(alg.alg_gauge, siter, eps)
+        psi = canonical_from_AL_keepAL(ALs, psi.C[N - 1], ag["tol"], ag["maxiter"])
+        ae = updatetol(alg.alg_environments, siter, eps)
+        envs = build_envs(psi, H, tol=ae["tol"], maxiter=ae["maxiter"], init=envs)
+        if alg.finalize is not None:
+            psi, envs = alg.finalize(it, psi, H, envs)
+        eps = calc_galerkin(psi, H, envs)
+        losses.append(eps)
+        if log is not None:
+            log.append(dict(iter=it, eps=eps, f=expectationvalue(psi, H, envs)))
+        if eps <= alg.tol:
+            converged = True
+            break
+    return psi, envs, dict(niter=it, converged=converged, losses=losses, itererr=losses[-1])
+
+
+def canonical_from_AL_keepAL(ALs, C0, tol, maxiter) -> CanonicalIMPS:
+    """``gauge_step!`` (``vumps.jl:257-266``): keep the candidate ``AL``, right gauge fix
+    from ``C0`` for ``AR, C``, then ``AC = AL C``."""
+    psi = gaugefix(ALs, C0, order="R", tol=tol, maxiter=maxiter)
+    psi.AC = [_mulAL(psi.AL[i], psi.C[i]) for i in range(len(ALs))]
+    return psi
+
+
+def timestep(psi: CanonicalIMPS, H: SchurMPO, dt: complex, alg: TDVP = None,
+             envs: Optional[DMRGCache] = None):
+    """``timestep(psi, H, dt, TDVP(), envs)`` (``src/algorithms/timeevo/tdvp.jl:34-53``)."""
+    alg = alg or TDVP()
+    if envs is None:
+        envs = build_envs(psi, H)
+    N = len(psi)
+    ig = alg.integrator
+    ACs, Cs = [], []
+    for loc in range(N):
+        GL, W, GR = envs.lefts[loc], H[loc], envs.rights[loc]
+        ac, _ = exponentiate(lambda x: ac_apply(GL, W, GR, x), dt, psi.AC[loc], ig["tol"], ig["krylovdim"], ig["maxiter"])
+        GLc = envs.lefts[(loc + 1) % N]
+        c, _ = exponentiate(lambda x: c_apply(GLc, GR, x), dt, psi.C[loc], ig["tol"], ig["krylovdim"], ig["maxiter"])
+        ACs.append(ac)
+        Cs.append(c)
+    ALs = [regauge(ACs[i], Cs[i]) for i in range(N)]
+    g = alg.alg_gauge.alg if isinstance(alg.alg_gauge, DynamicTol) else alg.alg_gauge
+    psi2 = canonical_from_AL(ALs, psi.C[N - 1], g["tol"], g["maxiter"])
+    envs2 = build_envs(psi2, H, init=envs)
+    return psi2, envs2
+
+
+def time_evolve(psi0: CanonicalIMPS, H: SchurMPO, t_span: Sequence[complex], alg: TDVP = None,
+                envs: Optional[DMRGCache] = None, observer: Optional[Callable] = None):
+    """``time_evolve`` (``tdvp.jl:91-113``)."""
+    alg = alg or TDVP()
+    psi = psi0.copy()
+    if envs is None:
+        envs = build_envs(psi, H)
+    hist = [observer(psi, 0, t_span[0]) if observer else expectationvalue(psi, H, envs)]
+    for it in range(1, len(t_span)):
+        dt = t_span[it] - t_span[it - 1]
+        psi, envs = timestep(psi, H, dt, alg, envs)
+        if alg.finalize is not None:
+            psi, envs = alg.finalize(t_span[it - 1], psi, H, envs)
+        hist.append(observer(psi, it, t_span[it]) if observer else expectationvalue(psi, H, envs))
+    return psi, envs, hist
+
+
+def idmrg_groundstate(psi0: CanonicalIMPS, H: SchurMPO, alg: IDMRG, envs: Optional[DMRGCache] = None):
+    """``find_groundstate(psi0, H, ::IDMRG)`` (``src/algorithms/groundstates/idmrg.jl:12-82``)."""
+    psi = psi0.copy()
+    N = len(psi)
+    if envs is None:
+        envs = build_envs(psi, H)
+    lefts = [x.copy(order="F") for x in envs.lefts]
+    rights = [x.copy(order="F") for x in envs.rights]
+    envs = DMRGCache(lefts, rights)
+    eps = calc_galerkin(psi, H, envs)
+    E = expectationvalue(psi, H, envs)
+    losses = [eps]
+    converged = False
+    it = 0
+    for it in range(1, alg.maxiter + 1):
+        ea = updatetol(alg.alg_eigsolve, it - 1, eps)
+        C_old = psi.C[N - 1].copy()
+        for pos in range(N):
+            GL, W, GR = envs.lefts[pos], H[pos], envs.rights[pos]
+            _, ac, _ = lanczos_eigsolve(lambda x: ac_apply(GL, W, GR, x), psi.AC[pos], ea["tol"],
+                                        ea["krylovdim"], ea["maxiter"], ea["eager"])
+            Dl, d, Dr = ac.shape
+            Q, R = qrpos(freshape(ac, (Dl * d, Dr)))
+            psi.AL[pos] = np.asfortranarray(freshape(Q, (Dl, d, Dr)))
+            psi.C[pos] = R
+            psi.AC[pos] = psi.AL[pos].copy(order="F") if pos != N - 1 else ac
+            nxt = (pos + 1) % N
+            envs.lefts[nxt] = push_mpo_left(envs.lefts[pos], H[pos], psi.AL[pos])
+        Enew = None
+        for pos in range(N - 1, -1, -1):
+            GL, W, GR = envs.lefts[pos], H[pos], envs.rights[pos]
+            Enew, ac, _ = lanczos_eigsolve(lambda x: ac_apply(GL, W, GR, x), psi.AC[pos], ea["tol"],
+                                           ea["krylovdim"], ea["maxiter"], ea["eager"])
+            Dl, d, Dr = ac.shape
+            Lf, Q = lqpos(freshape(ac, (Dl, d * Dr)))
+            psi.C[pos - 1] = Lf
+            psi.AR[pos] = np.asfortranarray(freshape(Q, (Dl, d, Dr)))
+            psi.AC[pos] = psi.AR[pos].copy(order="F") if pos != 0 else ac
+            prv = (pos - 1) % N
+            envs.rights[prv] = push_mpo_right(envs.rights[pos], H[pos], psi.AR[pos])
+        eps = _fnorm(psi.C[N - 1] - C_old)
+        losses.append(eps)
+        E = Enew
+        if eps <= alg.tol:
+            converged = True
+            break
+    ag = updatetol(alg.alg_gauge, it, eps)
+    psi2 = canonical_from_sites([psi.AR[l] for l in range(N)], tol=ag["tol"], maxiter=ag["maxiter"])
+    envs2 = build_envs(psi2, H, init=envs)
+    return psi2, envs2, dict(niter=it, converged=converged, losses=losses, itererr=losses[-1], E=E)
