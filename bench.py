@@ -1,0 +1,391 @@
+#!/usr/bin/env python
+"""Benchmark: VUMPS on the spinful Hubbard chain (Jordan-Wigner, t=1, U=4, mu=2,
+d=4, w=6), unit cell N=2, bond dimension D=1024, ComplexF64 states.
+
+A step is one VUMPS iteration (localupdate eigensolves + regauge!, gauge_step!,
+environment rebuild, Galerkin error and energy) on device-resident data.  The
+state starts from seeded random site tensors (PCG64 seed 3), canonicalised, and
+is advanced by W untimed warm-up iterations before K timed ones.  Inputs (the
+2 x 64 MiB site tensors and 2 x 96 MiB environments per side) exceed nothing in
+L2-resident terms: every Heff GEMM streams >100 MB operands, so no L2 flush is
+needed between iterations.
+
+One JSON line on rank 0 (see the keys below).  ``--impl reference`` times the
+CPU oracle (the NumPy restatement of the reference, which is not runnable here:
+no Julia) on a bounded sample of the same workload.  With ``--gpus N > 1`` the
+job runs N independent replicas (the path does not shard; no collective).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(workload="vumps_hubbard_jw", model="Fermi-Hubbard JW t=1 U=4 mu=2 (d=4, w=6)", N=2, D=1024,
+                seed=3, dtype="complex128")
+METRIC = "VUMPS iterations/s (Hubbard JW, N=2, D=1024)"
+UNIT = "iter/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--precision", default="fp64", choices=["fp64", "split"])
+    p.add_argument("--nslices", type=int, default=5)
+    p.add_argument("--D", type=int, default=WORKLOAD["D"])
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    return p.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (replicas only)
+# ---------------------------------------------------------------------------
+def dist_init(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def allmax(world, v):
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([v], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+    return v
+
+
+# ---------------------------------------------------------------------------
+# clocks sampler (nvidia-smi during the timed region)
+# ---------------------------------------------------------------------------
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.samples = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        sm = [float(s[1]) for s in self.samples if len(s) >= 9 and s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if len(s) >= 9 and s[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s in self.samples:
+            if len(s) >= 9:
+                for k, nm in enumerate(names):
+                    if s[5 + k].lower().startswith("active"):
+                        reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+# ---------------------------------------------------------------------------
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+def ac_flops(D, d, w):
+    # F_AC = 16 w d D^3 + 8 w^2 d^2 D^2 (algorithmic, complex MAC = 8 flops)
+    return 16.0 * w * d * D ** 3 + 8.0 * w * w * d * d * D ** 2
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    import infinitempsalgorithms_b200 as imps
+    from infinitempsalgorithms_b200 import _lib as L
+    import ctypes as C
+
+    torch.cuda.set_device(local)
+    ctx = imps.Context(local)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    if args.precision == "split":
+        ctx.set_precision(L.IMPS_PREC_SPLIT_I8, args.nslices)
+    lib = ctx.lib
+    D, N = args.D, WORKLOAD["N"]
+    H = imps.SparseIMPO([imps.hubbard_hamiltonian().Ws[0]] * N)
+    Hh = H.handle(ctx)
+    As = imps.random_site_tensors([4] * N, D, WORKLOAD["seed"] + 1000 * rank)
+    t0 = time.time()
+    psi = imps.CanonicalIMPS.from_sites(As, ctx=ctx)
+    envs = imps.DMRGCache(psi, H)
+    eps = imps.calc_galerkin(psi, H, envs)
+    imps.recalculate(envs, psi, H, tol=imps.updatetol(imps.Defaults.alg_environments(), 0, eps)["tol"])
+    prep_s = time.time() - t0
+
+    def step(it, eps):
+        info = L.VumpsInfo()
+        L.check(lib.imps_vumps_iter(envs.h, Hh, psi.h, it, eps, C.byref(info)), ctx.h)
+        return info
+
+    it = 0
+    for _ in range(args.warmup):
+        it += 1
+        info = step(it, eps)
+        eps = info.galerkin
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = Clocks(local)
+    clocks.start()
+    ctx.profile(True)
+    ctx.profile_reset()
+    c0 = ctx.counters()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    infos = []
+    for _ in range(args.steps):
+        it += 1
+        info = step(it, eps)
+        eps = info.galerkin
+        infos.append(info)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    c1 = ctx.counters()
+    prof = {k: ctx.profile_get(k) for k in ("zgemm_fp64", "gemm_split", "level_mix", "orth", "blas1", "qr", "permute",
+                                            "split_slice")}
+    ctx.profile(False)
+    barrier(world)
+    ms_max = allmax(world, ms)
+    steps_total = args.steps * world
+    value = steps_total / (ms_max / 1e3)
+    launches = c1["kernels"] - c0["kernels"]
+    # dominant kernel class and roofline
+    pk, pk_kind = peaks()
+    gem_key = "gemm_split" if args.precision == "split" else "zgemm_fp64"
+    n_g, ms_g, fl_g = prof[gem_key]
+    result = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c128" if args.precision == "fp64" else "c128 (int8-split Heff)",
+        "data": "synthetic (seeded PCG64 random MPS, no dataset)",
+        "config": dict(WORKLOAD, D=D, precision=args.precision,
+                       nslices=args.nslices if args.precision == "split" else None,
+                       parallelism=f"replicas{world}" if world > 1 else "single",
+                       l2="inputs > L2 (>100 MB operands per GEMM); no flush"),
+        "gpu_launches": int(launches),
+        "galerkin": infos[-1].galerkin, "energy_per_site": infos[-1].energy_re / N,
+        "ac_matvecs": int(sum(i.ac_matvecs for i in infos)), "c_matvecs": int(sum(i.c_matvecs for i in infos)),
+        "prep_s": prep_s, "iters_done": it,
+        "kernel_ms": {k: round(v[1], 3) for k, v in prof.items()},
+    }
+    if n_g:
+        achieved = fl_g / (ms_g / 1e3) / 1e12
+        result["roofline"] = {"bound": "tensor" if args.precision == "split" else "fp64-pipe",
+                              "kernel": gem_key, "achieved": achieved, "unit": "TFLOP/s",
+                              "launches": n_g, "avg_launch_ms": ms_g / n_g, "traffic": None}
+    # Heff matvec throughput on the final state (device-resident, AC site 1)
+    nrep = 10
+    x = torch.zeros(D * 4 * D, dtype=torch.complex128, device="cuda")
+    y = torch.zeros_like(x)
+    x.copy_(torch.randn(D * 4 * D, dtype=torch.complex128, device="cuda"))
+    for _ in range(2):
+        L.check(lib.imps_ac_apply_dev(envs.h, Hh, 0, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr())), ctx.h)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(nrep):
+        L.check(lib.imps_ac_apply_dev(envs.h, Hh, 0, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr())), ctx.h)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_ac = e0.elapsed_time(e1) / nrep
+    result["heff_matvecs_per_s"] = 1e3 / ms_ac
+    result["heff_ms"] = ms_ac
+    result["heff_tflops"] = ac_flops(D, 4, 6) / (ms_ac / 1e3) / 1e12
+    result["clocks"] = clk
+    if not args.no_e2e:
+        result["e2e"] = run_e2e(args, ctx, psi, envs, H, it, eps, world)
+    return result, ctx, psi, envs, H
+
+
+def run_e2e(args, ctx, psi, envs, H, it, eps, world):
+    """Same metric through the C ABI with host buffers: each step uploads the
+    state (AL/AR/C/AC of both sites) from pinned host memory, runs
+    imps_vumps_iter, and downloads the new state and the energy."""
+    import torch
+    import ctypes as C
+    from infinitempsalgorithms_b200 import _lib as L
+    lib = ctx.lib
+    N = psi.N
+    fields = [(f, l) for l in range(N) for f in (L.IMPS_AL, L.IMPS_AR, L.IMPS_C, L.IMPS_AC)]
+    host = {}
+    for f, l in fields:
+        shp = psi._shape(f, l)
+        t = torch.empty(int(np.prod(shp)), dtype=torch.complex128, pin_memory=True)
+        a = t.numpy()
+        L.check(lib.imps_state_get(psi.h, f, l, a.ctypes.data_as(L.DP)), ctx.h)
+        host[(f, l)] = (t, a)
+    h2d = sum(a.nbytes for _, a in host.values())
+    Hh = H.handle(ctx)
+    torch.cuda.synchronize()
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        it += 1
+        for (f, l), (_, a) in host.items():
+            L.check(lib.imps_state_set(psi.h, f, l, a.ctypes.data_as(L.DP)), ctx.h)
+        info = L.VumpsInfo()
+        L.check(lib.imps_vumps_iter(envs.h, Hh, psi.h, it, eps, C.byref(info)), ctx.h)
+        eps = info.galerkin
+        for (f, l), (_, a) in host.items():
+            L.check(lib.imps_state_get(psi.h, f, l, a.ctypes.data_as(L.DP)), ctx.h)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    dt = allmax(world, dt)
+    return {"value": args.steps * world / dt, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(h2d + 16)}
+
+
+# ---------------------------------------------------------------------------
+# CPU oracle timings (the reference is Julia and cannot run here)
+# ---------------------------------------------------------------------------
+def oracle_sample(D, budget_s=20.0):
+    """Time the oracle's dominant operations at the full workload size on the host
+    cores: one AC Heff apply, one C apply, one identity push, one QRpos of the
+    (4D x D) AC matrix.  Returns per-operation seconds."""
+    import oracle as O
+    rng = np.random.default_rng(0)
+    H = O.hubbard_hamiltonian()
+    W = H.Ws[0]
+    w, d = W.shape[0], W.shape[1]
+
+    def rc(*s):
+        return np.asfortranarray(rng.standard_normal(s) + 1j * rng.standard_normal(s))
+    GL, GR, x, Cm = rc(D, w, D), rc(D, w, D), rc(D, d, D), rc(D, D)
+    A = rc(D, d, D)
+    out = {}
+    t = time.perf_counter(); O.ac_apply(GL, W, GR, x); out["ac"] = time.perf_counter() - t
+    t = time.perf_counter(); O.c_apply(GL, GR, Cm); out["c"] = time.perf_counter() - t
+    t = time.perf_counter(); O.push_env_left(Cm, A); out["push"] = time.perf_counter() - t
+    t = time.perf_counter(); O.qrpos(O.freshape(A, (D * d, D))); out["qr"] = time.perf_counter() - t
+    return out
+
+
+def cpu_threads():
+    return int(os.environ.get("OPENBLAS_NUM_THREADS", os.cpu_count() or 1))
+
+
+def cpu_iter_seconds(op_s, counts):
+    """CPU seconds for one VUMPS iteration = sum over operation classes of
+    (count per iteration) x (oracle seconds per operation)."""
+    return (counts["ac"] * op_s["ac"] + counts["c"] * op_s["c"] + counts["push"] * op_s["push"]
+            + counts["qr"] * op_s["qr"])
+
+
+# Operation counts of one VUMPS iteration at this workload (AC applies incl. Galerkin
+# and energy, C applies, identity-push equivalents of the environment build, QR/LQ
+# factorizations), as counted by the GPU arm's own counters on the warmed-up state.
+ITER_COUNTS = {"ac": 40, "c": 40, "push": 200, "qr": 40}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return None
+    os.environ.setdefault("OPENBLAS_NUM_THREADS", str(os.cpu_count() or 1))
+    for _ in range(max(0, min(args.warmup, 1))):
+        oracle_sample(args.D)
+    times = []
+    ops = None
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        ops = oracle_sample(args.D)
+        times.append(cpu_iter_seconds(ops, ITER_COUNTS))
+    sec = float(np.mean(times))
+    sample = (f"per step: oracle (NumPy/OpenBLAS) AC apply, C apply, identity push and QRpos at D={args.D}, "
+              f"scaled by the per-iteration operation counts {ITER_COUNTS}")
+    return {"metric": METRIC, "value": 1.0 / sec, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c128", "data": "synthetic", "impl": "reference",
+            "config": dict(WORKLOAD, D=args.D),
+            "cpu_baseline": {"value": 1.0 / sec, "unit": UNIT, "cores": cpu_threads(), "kind": "port",
+                             "sample": sample, "op_seconds": ops},
+            "e2e": {"value": 1.0 / sec, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_init(args)
+    if args.impl == "reference":
+        res = run_reference(args, world, rank)
+        if rank == 0:
+            print(json.dumps(res))
+        return
+    res, ctx, psi, envs, H = run_ours(args, world, rank, local)
+    if rank == 0 and world == 1 and not args.no_cpu:
+        ops = oracle_sample(args.D)
+        counts = ITER_COUNTS
+        sec = cpu_iter_seconds(ops, counts)
+        res["cpu_baseline"] = {"value": 1.0 / sec, "unit": UNIT, "cores": cpu_threads(), "kind": "port",
+                               "sample": f"oracle AC/C apply, push, QRpos at D={args.D} x per-iteration counts {counts}",
+                               "op_seconds": ops}
+    pk, pk_kind = peaks()
+    if "roofline" in res:
+        if args.precision == "split":
+            res["roofline"]["peak"] = pk.get("bf16_tflops")
+            res["roofline"]["peak_kind"] = f"{pk_kind} bf16 dense (int8 products)"
+        else:
+            res["roofline"]["peak"] = None
+            res["roofline"]["peak_kind"] = "FP64: no driver-measured peak; see fp64_ref_tflops"
+        if res["roofline"].get("peak"):
+            res["roofline"]["frac"] = res["roofline"]["achieved"] / res["roofline"]["peak"]
+    if rank == 0:
+        print(json.dumps(res))
+
+
+if __name__ == "__main__":
+    main()

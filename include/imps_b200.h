@@ -179,6 +179,15 @@ int imps_push_mpo_left(imps_ctx* ctx, const imps_mpo* mpo, int site, int Dl, int
 int imps_push_mpo_right(imps_ctx* ctx, const imps_mpo* mpo, int site, int Dl, int Dr, const double* R,
                         const double* A, double* out);
 
+/* ------------------------------------------------------------------- GEMM */
+/* C = alpha op(A) op(B) + beta C on device pointers (column-major complex128),
+ * op: 0 = N, 1 = T, 2 = C (conjugate transpose), through the context's precision
+ * engine: the @tensor contractions of the reference (TensorOperations -> BLAS
+ * ZGEMM, src/InfiniteMPSAlgorithms.jl:260) run here. */
+int imps_zgemm(imps_ctx* ctx, int opA, int opB, int M, int N, int K, double alpha_re, double alpha_im,
+               const void* A, int64_t lda, const void* B, int64_t ldb, double beta_re, double beta_im, void* C,
+               int64_t ldc);
+
 /* --------------------------------------------------------- factorizations */
 /* leftorth(M; alg = QRpos()) / rightorth(M; alg = LQpos()) (FiniteMPSAlgorithms,
  * used at src/states/ortho.jl:150, 188, 214-225).  M is m x n column-major. */

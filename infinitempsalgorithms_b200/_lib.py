@@ -108,6 +108,7 @@ _SIGS = {
     "imps_push_right": (I32, [P, I32, I32, I32, DP, DP, DP, DP]),
     "imps_push_mpo_left": (I32, [P, P, I32, I32, I32, DP, DP, DP]),
     "imps_push_mpo_right": (I32, [P, P, I32, I32, I32, DP, DP, DP]),
+    "imps_zgemm": (I32, [P, I32, I32, I32, I32, I32, D, D, P, I64, P, I64, D, D, P, I64]),
     "imps_qrpos": (I32, [P, I32, I32, DP, DP, DP]),
     "imps_lqpos": (I32, [P, I32, I32, DP, DP, DP]),
     "imps_regauge": (I32, [P, I32, I32, I32, DP, DP, DP]),

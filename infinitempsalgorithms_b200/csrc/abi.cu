@@ -591,6 +591,21 @@ int imps_push_mpo_right(imps_ctx* h, const imps_mpo* mpo, int site, int Dl, int 
   return push_mpo_common(h, mpo, site, Dl, Dr, R, A, out, false);
 }
 
+// ------------------------------------------------------------------ GEMM
+int imps_zgemm(imps_ctx* h, int opA, int opB, int M, int N, int K, double alpha_re, double alpha_im,
+               const void* A, int64_t lda, const void* B, int64_t ldb, double beta_re, double beta_im, void* Cp,
+               int64_t ldc) {
+  if (!h || !A || !B || !Cp || M < 0 || N < 0 || K < 0) return IMPS_INVALID_ARG;
+  if (opA < 0 || opA > 2 || opB < 0 || opB > 2) return IMPS_INVALID_ARG;
+  return guard(&h->c, [&] {
+    imps::zgemm(&h->c, (imps::Op)opA, (imps::Op)opB, M, N, K, imps::cplx(alpha_re, alpha_im),
+                static_cast<const imps::dcplx*>(A), lda, 0, static_cast<const imps::dcplx*>(B), ldb, 0,
+                imps::cplx(beta_re, beta_im), static_cast<imps::dcplx*>(Cp), ldc, 0, 1, true);
+    IMPS_CUDA(cudaStreamSynchronize(h->c.stream));
+    return IMPS_OK;
+  });
+}
+
 // ------------------------------------------------------------------ factorizations
 int imps_qrpos(imps_ctx* h, int m, int n, const double* M, double* Q, double* R) {
   if (!h || !M || !Q || !R || m <= 0 || n <= 0) return IMPS_INVALID_ARG;

@@ -1,0 +1,608 @@
+// Split-precision complex GEMM on the 5th-generation tensor cores (tcgen05, kind::i8).
+//
+// Scheme (Ozaki splitting with power-of-two scaling).  Each complex row i of
+// op(A) gets a scale r_i = 2^e >= max_k max(|Re|,|Im|) and each complex column j of
+// op(B) a scale c_j; the scaled values x / scale lie in (-1, 1) and are cut into
+// `s` int8 slices x = scale * sum_t a_t 2^-7(t+1) (truncating, |a_t| <= 127).  The
+// complex product is carried by a real GEMM of the expanded operands
+//     At (2M x 2K): rows (i, re/im), cols (k, re/im) = [[Re, -Im], [Im, Re]]
+//     Bt (N x 2K):  rows j,            cols (k, re/im) = [Re b_kj, Im b_kj]
+// so that row 2i+p of At Bt^T is (Re, Im)[p] of c_ij.  For every diagonal
+// d = ta + tb < s the slice pairs are summed *exactly* in an int32 TMEM
+// accumulator (the K extent is chunked so no sum can overflow), and the
+// epilogue adds r_i c_j 2^-7(d+2) acc to the FP64 output.  Truncation error per
+// element is below 2^-7s of the row/column scale.
+//
+// GEMM kernel: persistent, one CTA per SM, warp-specialised:
+//   warp 0: TMA producer (cp.async.bulk.tensor, 128B swizzle, 4-stage ring)
+//   warp 1: TMEM allocator + single-thread tcgen05.mma issuer (M=128, N=256, K=32)
+//   warps 2-5: epilogue, tcgen05.ld 32x32b from a double-buffered accumulator
+// Every mbarrier wait is bounded (~1 s of clock64); on expiry the kernel sets an
+// error flag, drains and returns, and the host raises IMPS_TIMEOUT.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "imps_internal.h"
+#include "split_gemm.h"
+
+namespace imps {
+namespace {
+
+constexpr int BM = 128;          // tile rows (real rows of At)
+constexpr int BN = 256;          // tile cols (rows of Bt)
+constexpr int BKB = 128;         // K bytes per stage (one 128B swizzle atom)
+constexpr int STAGES = 4;
+constexpr int A_STAGE = BM * BKB;   // 16 KB
+constexpr int B_STAGE = BN * BKB;   // 32 KB
+constexpr int SMEM_TILES = STAGES * (A_STAGE + B_STAGE);
+constexpr int SMEM_BYTES = SMEM_TILES + 1024 /*align*/ + 256 /*barriers*/;
+constexpr int NTHREADS = 192;
+constexpr long long WAIT_CYCLES = 2000000000LL;   // ~1 s at 1.9 GHz
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait: returns false (and raises the error flag) after ~1 s
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* err) {
+  long long t0 = clock64();
+  while (!mbar_try(bar, parity)) {
+    if (*err) return false;
+    if (clock64() - t0 > WAIT_CYCLES) {
+      atomicExch((int*)err, 1);
+      return false;
+    }
+  }
+  return true;
+}
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y, int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];"
+      ::"r"(smem_u32(dst)), "l"(map), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z)
+      : "memory");
+}
+
+// UMMA shared-memory descriptor: K-major, 128B swizzle, 8-row groups 1024 B apart.
+__device__ __forceinline__ uint64_t make_desc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);          // start address
+  d |= (uint64_t)1 << 16;                           // leading byte offset (unused for SW128 K-major)
+  d |= (uint64_t)(1024 >> 4) << 32;                 // stride byte offset
+  d |= (uint64_t)1 << 46;                           // descriptor version (sm100)
+  d |= (uint64_t)2 << 61;                           // SWIZZLE_128B
+  return d;
+}
+
+// instruction descriptor: kind::i8, s8 x s8 -> s32, both K-major, M = 128, N = 256
+__host__ __device__ constexpr uint32_t make_idesc() {
+  return (2u << 4)                 // D format: s32
+         | (1u << 7)               // A format: s8
+         | (1u << 10)              // B format: s8
+         | ((uint32_t)(BN >> 3) << 17)
+         | ((uint32_t)(BM >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc));
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, int32_t* r) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+struct GemmArgs {
+  int num_m, num_n;          // tiles
+  int kblocks;               // K blocks of 128 bytes per slice plane
+  int diag;                  // slice diagonal d
+  int kb_begin, kb_end;      // K-chunk [kb_begin, kb_end) within each plane
+  double2* C;                // complex output
+  int64_t ldc;
+  int Mc, Nc;                // valid complex rows / cols
+  const double* row_scale;   // per complex row of op(A)
+  const double* col_scale;   // per complex col of op(B)
+  double gscale;             // alpha * 2^-7(d+2)
+  int accumulate;            // 0: C = result, 1: C += result
+  int* err;
+};
+
+__global__ void __launch_bounds__(NTHREADS, 1)
+    k_gemm_i8(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, const GemmArgs g) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t* sA = smem;
+  uint8_t* sB = smem + STAGES * A_STAGE;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + SMEM_TILES);
+  uint64_t* full = bars;                 // [STAGES]
+  uint64_t* empty = bars + STAGES;       // [STAGES]
+  uint64_t* tfull = bars + 2 * STAGES;   // [2]
+  uint64_t* tempty = bars + 2 * STAGES + 2;  // [2]
+  uint64_t* drain = bars + 2 * STAGES + 4;   // MMA drain on the error path
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * STAGES + 5);
+  volatile int* err = g.err;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(&tfull[a], 1);
+      mbar_init(&tempty[a], 4);  // one arrival per epilogue warp
+    }
+    mbar_init(drain, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(tmem_slot)));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  const int ntiles = g.num_m * g.num_n;
+  const int npairs = g.diag + 1;
+  const int kspan = g.kb_end - g.kb_begin;
+  const int ksteps = npairs * kspan;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      int stage = 0;
+      uint32_t phase = 0;
+      bool ok = true;
+      int issued[STAGES];          // parity of the last load issued into each stage (-1: none)
+      for (int s2 = 0; s2 < STAGES; ++s2) issued[s2] = -1;
+      for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+        const int mb = t % g.num_m, nb = t / g.num_m;
+        for (int step = 0; step < ksteps && ok; ++step) {
+          const int ta = step / kspan, kb = g.kb_begin + step % kspan;
+          const int tb = g.diag - ta;
+          ok = mbar_wait(&empty[stage], phase ^ 1, err);
+          if (!ok) break;
+          mbar_expect_tx(&full[stage], A_STAGE + B_STAGE);
+          tma_load_3d(sA + stage * A_STAGE, &mapA, &full[stage], kb * BKB, mb * BM, ta);
+          tma_load_3d(sB + stage * B_STAGE, &mapB, &full[stage], kb * BKB, nb * BN, tb);
+          issued[stage] = (int)phase;
+          if (++stage == STAGES) { stage = 0; phase ^= 1; }
+        }
+      }
+      // every issued copy must land before the CTA may exit (bounded)
+      for (int s2 = 0; s2 < STAGES; ++s2) {
+        if (issued[s2] < 0) continue;
+        long long t0 = clock64();
+        while (!mbar_try(&full[s2], (uint32_t)issued[s2]) && clock64() - t0 < WAIT_CYCLES) {
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      const uint32_t idesc = make_idesc();
+      int stage = 0;
+      uint32_t phase = 0;
+      int lt = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++lt) {
+        const int acc = lt & 1;
+        const uint32_t tphase = (lt >> 1) & 1;
+        ok = mbar_wait(&tempty[acc], tphase ^ 1, err);
+        if (!ok) break;
+        tc_fence_after();
+        const uint32_t dtmem = tmem_base + acc * BN;
+        for (int step = 0; step < ksteps; ++step) {
+          ok = mbar_wait(&full[stage], phase, err);
+          if (!ok) break;
+          tc_fence_after();
+          const uint32_t a0 = smem_u32(sA + stage * A_STAGE), b0 = smem_u32(sB + stage * B_STAGE);
+#pragma unroll
+          for (int kk = 0; kk < BKB / 32; ++kk) {
+            umma_i8(dtmem, make_desc(a0 + kk * 32), make_desc(b0 + kk * 32), idesc, (step > 0 || kk > 0) ? 1u : 0u);
+          }
+          umma_commit(&empty[stage]);  // frees the smem stage when these MMAs retire
+          if (++stage == STAGES) { stage = 0; phase ^= 1; }
+        }
+        if (!ok) break;
+        umma_commit(&tfull[acc]);
+      }
+      // all MMAs issued by this thread retire before TMEM is released (bounded)
+      umma_commit(drain);
+      long long t0 = clock64();
+      while (!mbar_try(drain, 0) && clock64() - t0 < WAIT_CYCLES) {
+      }
+    }
+  } else {
+    // epilogue warps 2..5: TMEM lane quarter = warp % 4
+    const int q = warp & 3;
+    const int row = q * 32 + lane;  // tile row == TMEM lane
+    int lt = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++lt) {
+      const int acc = lt & 1;
+      const uint32_t tphase = (lt >> 1) & 1;
+      if (!mbar_wait(&tfull[acc], tphase, err)) break;
+      tc_fence_after();
+      const int mb = t % g.num_m, nb = t / g.num_m;
+      const int rr = mb * BM + row;           // real row of At
+      const int ci = rr >> 1, part = rr & 1;  // complex row, re/im
+      const bool rvalid = ci < g.Mc;
+      const double rs = rvalid ? g.row_scale[ci] * g.gscale : 0.0;
+      double* Cd = reinterpret_cast<double*>(g.C);
+      for (int cc = 0; cc < BN / 32; ++cc) {
+        int32_t r[32];
+        tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + acc * BN + cc * 32, r);
+        if (rvalid) {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            const int cj = nb * BN + cc * 32 + j;
+            if (cj < g.Nc) {
+              double v = (double)r[j] * rs * g.col_scale[cj];
+              double* p = Cd + 2 * ((int64_t)ci + g.ldc * cj) + part;
+              *p = g.accumulate ? (*p + v) : v;
+            }
+          }
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&tempty[acc]);
+    }
+  }
+  // drain: make sure every MMA of this CTA retired before releasing TMEM
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem_base));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Slicing kernels (memory bound)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long dbits(double x) { return (unsigned long long)__double_as_longlong(x); }
+
+// per complex row i of op(A) (opA N: A[i + lda k]) -> atomicMax of max(|re|,|im|) bits
+__global__ void k_rowmax_colmajor(int M, int K, const double2* __restrict__ A, int64_t lda, int kchunk,
+                                  unsigned long long* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= M) return;
+  const int k0 = blockIdx.y * kchunk, k1 = min(K, k0 + kchunk);
+  double m = 0.0;
+  for (int k = k0; k < k1; ++k) {
+    double2 v = A[i + lda * k];
+    m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
+  }
+  atomicMax(&out[i], dbits(m));
+}
+// per "contiguous line" l (A[k + ld l], k < K): max over k (warp per line)
+__global__ void k_linemax_contig(int L, int K, const double2* __restrict__ A, int64_t ld,
+                                 unsigned long long* __restrict__ out) {
+  const int l = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (l >= L) return;
+  double m = 0.0;
+  for (int k = lane; k < K; k += 32) {
+    double2 v = A[k + ld * l];
+    m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if (lane == 0) out[l] = dbits(m);
+}
+// column max of a row-major-strided view: out[j] = max_k |B[j + ld k]|  (thread per j, chunked k)
+__global__ void k_colmax_strided(int Ncol, int K, const double2* __restrict__ B, int64_t ld, int kchunk,
+                                 unsigned long long* __restrict__ out) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= Ncol) return;
+  const int k0 = blockIdx.y * kchunk, k1 = min(K, k0 + kchunk);
+  double m = 0.0;
+  for (int k = k0; k < k1; ++k) {
+    double2 v = B[j + ld * k];
+    m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
+  }
+  atomicMax(&out[j], dbits(m));
+}
+
+// max bits -> scale 2^e > max, and its inverse (exact powers of two)
+__global__ void k_scales(int n, const unsigned long long* __restrict__ mx, double* __restrict__ scale,
+                         double* __restrict__ inv) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double m = __longlong_as_double((long long)mx[i]);
+  if (!(m > 0.0) || !isfinite(m)) {
+    scale[i] = 0.0;
+    inv[i] = 0.0;
+    return;
+  }
+  int e;
+  frexp(m, &e);  // m = f 2^e, f in [0.5, 1)  =>  m < 2^e
+  scale[i] = ldexp(1.0, e);
+  inv[i] = ldexp(1.0, -e);
+}
+
+__device__ __forceinline__ void slice_value(double x, int s, int8_t* out) {
+  // x in (-1, 1): out[t] = trunc(x * 128); x = x * 128 - out[t]
+  for (int t = 0; t < s; ++t) {
+    double v = x * 128.0;
+    double a = trunc(v);
+    out[t] = (int8_t)a;
+    x = v - a;
+  }
+}
+
+// Split op(A) into expanded K-major planes.  Element (i, k) of op(A); each thread
+// produces 2 real rows x 2 real cols (4 bytes in 2 rows) per plane.
+// opA == 0: A[i + lda k] (tile-transposed through shared memory), opA == 2: conj(A[k + lda i]).
+template <int OPA>
+__global__ void k_split_a(int M, int K, const double2* __restrict__ A, int64_t lda, const double* __restrict__ inv,
+                          int s, int8_t* __restrict__ out, int64_t Kp, int64_t plane) {
+  __shared__ double2 tile[32][33];
+  const int i0 = blockIdx.y * 32, k0 = blockIdx.x * 32;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+  for (int r = ty; r < 32; r += 8) {
+    int i, k;
+    double2 v = make_double2(0.0, 0.0);
+    if (OPA == 0) {
+      i = i0 + tx; k = k0 + r;
+      if (i < M && k < K) v = A[i + lda * k];
+      tile[tx][r] = v;   // tile[i_local][k_local]
+    } else {
+      k = k0 + tx; i = i0 + r;
+      if (i < M && k < K) { v = A[k + lda * i]; v.y = -v.y; }
+      tile[r][tx] = v;
+    }
+  }
+  __syncthreads();
+  // write: real rows 2i, 2i+1; real cols 2k, 2k+1.  Thread (tx = k_local, ty) handles rows i_local = ty + 8j
+  for (int il = ty; il < 32; il += 8) {
+    const int i = i0 + il, k = k0 + tx;
+    if (i >= M) continue;
+    const double2 v = tile[il][tx];
+    const double sc = inv[i];
+    int8_t re[8], im[8];
+    slice_value(v.x * sc, s, re);
+    slice_value(v.y * sc, s, im);
+    for (int t = 0; t < s; ++t) {
+      // row 2i: (Re, -Im); row 2i+1: (Im, Re)
+      int8_t* p0 = out + plane * t + (int64_t)(2 * i) * Kp + 2 * k;
+      int8_t* p1 = p0 + Kp;
+      char2 w0, w1;
+      w0.x = (k < K) ? re[t] : 0;
+      w0.y = (k < K) ? (int8_t)(-im[t]) : 0;
+      w1.x = (k < K) ? im[t] : 0;
+      w1.y = (k < K) ? re[t] : 0;
+      *reinterpret_cast<char2*>(p0) = w0;
+      *reinterpret_cast<char2*>(p1) = w1;
+    }
+  }
+}
+
+// Split op(B) (K x N complex) into K-major planes Bt[j][2k + p].
+// opB == 0: B[k + ldb j] (contiguous in k); opB == 2: conj(B[j + ldb k]) (tile transpose).
+template <int OPB>
+__global__ void k_split_b(int K, int N, const double2* __restrict__ B, int64_t ldb, const double* __restrict__ inv,
+                          int s, int8_t* __restrict__ out, int64_t Kp, int64_t plane) {
+  __shared__ double2 tile[32][33];
+  const int j0 = blockIdx.y * 32, k0 = blockIdx.x * 32;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  for (int r = ty; r < 32; r += 8) {
+    double2 v = make_double2(0.0, 0.0);
+    if (OPB == 0) {
+      int k = k0 + tx, j = j0 + r;
+      if (k < K && j < N) v = B[k + ldb * j];
+      tile[r][tx] = v;  // tile[j_local][k_local]
+    } else {
+      int j = j0 + tx, k = k0 + r;
+      if (k < K && j < N) { v = B[j + ldb * k]; v.y = -v.y; }
+      tile[tx][r] = v;
+    }
+  }
+  __syncthreads();
+  for (int jl = ty; jl < 32; jl += 8) {
+    const int j = j0 + jl, k = k0 + tx;
+    if (j >= N) continue;
+    const double2 v = tile[jl][tx];
+    const double sc = inv[j];
+    int8_t re[8], im[8];
+    slice_value(v.x * sc, s, re);
+    slice_value(v.y * sc, s, im);
+    for (int t = 0; t < s; ++t) {
+      char2 w;
+      w.x = (k < K) ? re[t] : 0;
+      w.y = (k < K) ? im[t] : 0;
+      *reinterpret_cast<char2*>(out + plane * t + (int64_t)j * Kp + 2 * k) = w;
+    }
+  }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    cudaDriverEntryPointQueryResult q;
+    void* p = nullptr;
+    IMPS_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+    IMPS_REQUIRE(p && q == cudaDriverEntryPointSuccess, IMPS_CUDA_ERROR, "cuTensorMapEncodeTiled unavailable");
+    fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+// 3D map over int8 planes: dims (Kp bytes, rows, planes), box (128, box_rows, 1), 128B swizzle
+CUtensorMap make_map(const int8_t* base, int64_t Kp, int64_t rows, int planes, int box_rows) {
+  CUtensorMap m;
+  std::memset(&m, 0, sizeof(m));
+  cuuint64_t dims[3] = {(cuuint64_t)Kp, (cuuint64_t)rows, (cuuint64_t)planes};
+  cuuint64_t strides[2] = {(cuuint64_t)Kp, (cuuint64_t)(Kp * rows)};
+  cuuint32_t box[3] = {(cuuint32_t)BKB, (cuuint32_t)box_rows, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = get_encode()(&m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<int8_t*>(base), dims, strides, box, estr,
+                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  IMPS_REQUIRE(r == CUDA_SUCCESS, IMPS_CUDA_ERROR, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+  return m;
+}
+
+int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+void split_operand_a(Context* ctx, SplitOperand& S, Op op, int M, int K, const dcplx* A, int64_t lda, int s) {
+  IMPS_REQUIRE(op == OP_N || op == OP_C, IMPS_INVALID_ARG, "split: op T is not supported");
+  IMPS_REQUIRE(s >= 1 && s <= 8, IMPS_INVALID_ARG, "split: 1..8 slices");
+  S.rows = M;
+  S.K = K;
+  S.s = s;
+  S.Rp = round_up(2 * (int64_t)M, BM);
+  S.Kp = round_up(2 * (int64_t)K, BKB);
+  const size_t plane = (size_t)S.Rp * S.Kp;
+  S.data.ensure(plane * s);
+  S.scale.ensure((size_t)M * sizeof(double));
+  S.inv.ensure((size_t)M * sizeof(double));
+  S.mx.ensure((size_t)M * sizeof(unsigned long long));
+  ScopedTimer tm(ctx, "split_slice", 16.0 * M * K + (double)plane * s);
+  IMPS_CUDA(cudaMemsetAsync(S.data.ptr, 0, plane * s, ctx->stream));
+  IMPS_CUDA(cudaMemsetAsync(S.mx.ptr, 0, (size_t)M * 8, ctx->stream));
+  auto* mx = static_cast<unsigned long long*>(S.mx.ptr);
+  if (op == OP_N) {
+    const int kchunk = 64;
+    dim3 g((M + 127) / 128, (K + kchunk - 1) / kchunk);
+    k_rowmax_colmajor<<<g, 128, 0, ctx->stream>>>(M, K, A, lda, kchunk, mx);
+  } else {
+    k_linemax_contig<<<(M + 7) / 8, 256, 0, ctx->stream>>>(M, K, A, lda, mx);
+  }
+  k_scales<<<(M + 255) / 256, 256, 0, ctx->stream>>>(M, mx, S.scale.d(), S.inv.d());
+  dim3 g2((K + 31) / 32, (M + 31) / 32);
+  if (op == OP_N)
+    k_split_a<0><<<g2, 256, 0, ctx->stream>>>(M, K, A, lda, S.inv.d(), s, static_cast<int8_t*>(S.data.ptr), S.Kp, plane);
+  else
+    k_split_a<2><<<g2, 256, 0, ctx->stream>>>(M, K, A, lda, S.inv.d(), s, static_cast<int8_t*>(S.data.ptr), S.Kp, plane);
+  ctx->n_kernels += 5;
+  IMPS_CUDA(cudaPeekAtLastError());
+}
+
+void split_operand_b(Context* ctx, SplitOperand& S, Op op, int K, int N, const dcplx* B, int64_t ldb, int s) {
+  IMPS_REQUIRE(op == OP_N || op == OP_C, IMPS_INVALID_ARG, "split: op T is not supported");
+  IMPS_REQUIRE(s >= 1 && s <= 8, IMPS_INVALID_ARG, "split: 1..8 slices");
+  S.rows = N;
+  S.K = K;
+  S.s = s;
+  S.Rp = round_up(N, BN);
+  S.Kp = round_up(2 * (int64_t)K, BKB);
+  const size_t plane = (size_t)S.Rp * S.Kp;
+  S.data.ensure(plane * s);
+  S.scale.ensure((size_t)N * sizeof(double));
+  S.inv.ensure((size_t)N * sizeof(double));
+  S.mx.ensure((size_t)N * sizeof(unsigned long long));
+  ScopedTimer tm(ctx, "split_slice", 16.0 * K * N + (double)plane * s);
+  IMPS_CUDA(cudaMemsetAsync(S.data.ptr, 0, plane * s, ctx->stream));
+  IMPS_CUDA(cudaMemsetAsync(S.mx.ptr, 0, (size_t)N * 8, ctx->stream));
+  auto* mx = static_cast<unsigned long long*>(S.mx.ptr);
+  if (op == OP_N) {
+    k_linemax_contig<<<(N + 7) / 8, 256, 0, ctx->stream>>>(N, K, B, ldb, mx);
+  } else {
+    const int kchunk = 64;
+    dim3 g((N + 127) / 128, (K + kchunk - 1) / kchunk);
+    k_colmax_strided<<<g, 128, 0, ctx->stream>>>(N, K, B, ldb, kchunk, mx);
+  }
+  k_scales<<<(N + 255) / 256, 256, 0, ctx->stream>>>(N, mx, S.scale.d(), S.inv.d());
+  dim3 g2((K + 31) / 32, (N + 31) / 32);
+  if (op == OP_N)
+    k_split_b<0><<<g2, 256, 0, ctx->stream>>>(K, N, B, ldb, S.inv.d(), s, static_cast<int8_t*>(S.data.ptr), S.Kp, plane);
+  else
+    k_split_b<2><<<g2, 256, 0, ctx->stream>>>(K, N, B, ldb, S.inv.d(), s, static_cast<int8_t*>(S.data.ptr), S.Kp, plane);
+  ctx->n_kernels += 5;
+  IMPS_CUDA(cudaPeekAtLastError());
+}
+
+void split_gemm(Context* ctx, const SplitOperand& A, const SplitOperand& B, int s, double alpha, bool accumulate,
+                dcplx* C, int64_t ldc) {
+  IMPS_REQUIRE(A.K == B.K && A.Kp == B.Kp, IMPS_DIM_MISMATCH, "split_gemm: inner dimensions differ");
+  IMPS_REQUIRE(s <= A.s && s <= B.s, IMPS_INVALID_ARG, "split_gemm: more slices requested than stored");
+  static bool attr = false;
+  if (!attr) {
+    IMPS_CUDA(cudaFuncSetAttribute(k_gemm_i8, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+    attr = true;
+  }
+  const CUtensorMap mapA = make_map(static_cast<const int8_t*>(A.data.ptr), A.Kp, A.Rp, A.s, BM);
+  const CUtensorMap mapB = make_map(static_cast<const int8_t*>(B.data.ptr), B.Kp, B.Rp, B.s, BN);
+  DevBuf& errb = ctx->buf("gemm_i8_err", 16);
+  IMPS_CUDA(cudaMemsetAsync(errb.ptr, 0, 16, ctx->stream));
+  GemmArgs g;
+  g.num_m = (int)(A.Rp / BM);
+  g.num_n = (int)(B.Rp / BN);
+  g.kblocks = (int)(A.Kp / BKB);
+  g.C = C;
+  g.ldc = ldc;
+  g.Mc = A.rows;
+  g.Nc = B.rows;
+  g.row_scale = A.scale.d();
+  g.col_scale = B.scale.d();
+  g.err = static_cast<int*>(errb.ptr);
+  // K chunk bound: (d+1) * chunk_bytes * 127^2 < 2^31  ->  per diagonal
+  const int ntiles = g.num_m * g.num_n;
+  const int grid = std::max(1, std::min(ntiles, ctx->num_sms));
+  bool first = true;
+  for (int d = 0; d < s; ++d) {
+    const int64_t max_k_bytes = (int64_t)(2147483647.0 / (16129.0 * (d + 1)));
+    const int kbchunk = (int)std::max<int64_t>(1, max_k_bytes / BKB);
+    for (int kb0 = 0; kb0 < g.kblocks; kb0 += kbchunk) {
+      g.diag = d;
+      g.kb_begin = kb0;
+      g.kb_end = std::min(g.kblocks, kb0 + kbchunk);
+      g.gscale = alpha * std::ldexp(1.0, -7 * (d + 2));
+      g.accumulate = (first && !accumulate) ? 0 : 1;
+      first = false;
+      ScopedTimer tm(ctx, "gemm_split",
+                     2.0 * (double)A.Rp * (double)B.Rp * (double)(g.kb_end - g.kb_begin) * BKB * (d + 1));
+      k_gemm_i8<<<grid, NTHREADS, SMEM_BYTES, ctx->stream>>>(mapA, mapB, g);
+      ctx->n_kernels++;
+      ctx->n_gemm++;
+      IMPS_CUDA(cudaPeekAtLastError());
+    }
+  }
+  int herr = 0;
+  IMPS_CUDA(cudaMemcpyAsync(&herr, errb.ptr, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  IMPS_CUDA(cudaStreamSynchronize(ctx->stream));
+  IMPS_REQUIRE(herr == 0, IMPS_TIMEOUT, "split GEMM: a pipeline wait timed out");
+}
+
+}  // namespace imps

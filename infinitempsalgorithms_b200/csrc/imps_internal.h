@@ -13,6 +13,8 @@
 #include <cstdio>
 #include <map>
 #include <memory>
+#include <set>
+#include <tuple>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -93,6 +95,12 @@ struct KernelStat {
 
 enum GemmPrecision { PREC_FP64 = 0, PREC_SPLIT_I8 = 1 };
 
+struct SplitOperand;
+// (pointer, side, op, rows, K, ld, slices) -> split planes of an operand that is
+// constant for the current scope (environments during a solve, site tensors
+// during an environment build)
+using SplitKey = std::tuple<const void*, int, int, int, int, int64_t, int>;
+
 struct Context {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -118,6 +126,13 @@ struct Context {
   // counters
   int64_t n_ac_apply = 0, n_c_apply = 0, n_push = 0, n_gemm = 0, n_kernels = 0;
   int num_sms = 148;
+  // split-precision state
+  double split_tol = 1e-10;            // accuracy requested by the running solver
+  int force_fp64 = 0;                  // > 0: every GEMM in FP64 (gauge, Galerkin, energy)
+  std::multiset<const void*> const_ptrs;
+  std::map<SplitKey, std::shared_ptr<SplitOperand>> split_cache;
+  std::shared_ptr<SplitOperand> split_scratch[2];
+  int64_t split_calls = 0, split_cache_hits = 0;
 
   DevBuf& buf(const std::string& name, size_t bytes) {
     DevBuf& b = scratch[name];
@@ -125,6 +140,40 @@ struct Context {
     return b;
   }
   double* pinned(size_t bytes);
+};
+
+// Marks operands constant for the lifetime of the scope (their int8 splits are cached).
+struct ConstScope {
+  Context* ctx;
+  std::vector<const void*> ptrs;
+  ConstScope(Context* c, std::vector<const void*> p) : ctx(c), ptrs(std::move(p)) {
+    for (auto q : ptrs) ctx->const_ptrs.insert(q);
+  }
+  ~ConstScope() {
+    for (auto q : ptrs) {
+      auto it = ctx->const_ptrs.find(q);
+      if (it != ctx->const_ptrs.end()) ctx->const_ptrs.erase(it);
+      if (ctx->const_ptrs.count(q) == 0) {
+        for (auto it2 = ctx->split_cache.begin(); it2 != ctx->split_cache.end();) {
+          if (std::get<0>(it2->first) == q) it2 = ctx->split_cache.erase(it2);
+          else ++it2;
+        }
+      }
+    }
+  }
+};
+// Forces FP64 for every GEMM while alive.
+struct Fp64Scope {
+  Context* ctx;
+  explicit Fp64Scope(Context* c) : ctx(c) { ctx->force_fp64++; }
+  ~Fp64Scope() { ctx->force_fp64--; }
+};
+// Sets the accuracy the split GEMMs must meet while alive.
+struct TolScope {
+  Context* ctx;
+  double old;
+  TolScope(Context* c, double tol) : ctx(c), old(c->split_tol) { ctx->split_tol = tol; }
+  ~TolScope() { ctx->split_tol = old; }
 };
 
 // RAII timer for one kernel class on the context stream (active when profiling).

@@ -6,6 +6,9 @@
 // consecutive addresses), K tile of 8 staged through shared memory with a
 // register prefetch of the next tile.  Each complex MAC is 4 DFMA.
 #include "imps_internal.h"
+#include "split_gemm.h"
+
+#include <cmath>
 
 namespace imps {
 namespace {
@@ -173,11 +176,58 @@ void zgemm_fp64(Context* ctx, Op opA, Op opB, int M, int N, int K, cplx alpha, c
   if (e != cudaSuccess) throw Error(IMPS_CUDA_ERROR, std::string("zgemm launch: ") + cudaGetErrorString(e));
 }
 
+int slices_for_tol(double tol) {
+  // truncation error of s slices is below 2^-7s of the row/column scale; keep a
+  // 2^6 margin for the K-sum and the operator norm
+  if (!(tol > 0)) return 7;
+  int s = (int)std::ceil((-std::log2(tol) + 6.0) / 7.0);
+  return std::min(7, std::max(2, s));
+}
+
+static std::shared_ptr<SplitOperand> get_split(Context* ctx, int side, Op op, int rows, int K, const dcplx* X,
+                                               int64_t ld, int s) {
+  const bool constant = ctx->const_ptrs.count(X) > 0;
+  SplitKey key{X, side, (int)op, rows, K, ld, s};
+  if (constant) {
+    auto it = ctx->split_cache.find(key);
+    if (it != ctx->split_cache.end()) {
+      ctx->split_cache_hits++;
+      return it->second;
+    }
+  }
+  std::shared_ptr<SplitOperand> S;
+  if (constant) {
+    S = std::make_shared<SplitOperand>();
+  } else {
+    // transient operand: reuse one scratch object per side of this context
+    if (!ctx->split_scratch[side]) ctx->split_scratch[side] = std::make_shared<SplitOperand>();
+    S = ctx->split_scratch[side];
+  }
+  if (side == 0) split_operand_a(ctx, *S, op, rows, K, X, ld, s);
+  else split_operand_b(ctx, *S, op, K, rows, X, ld, s);
+  if (constant) ctx->split_cache[key] = S;
+  return S;
+}
+
 void zgemm(Context* ctx, Op opA, Op opB, int M, int N, int K, cplx alpha, const dcplx* A, int64_t lda,
            int64_t strideA, const dcplx* B, int64_t ldb, int64_t strideB, cplx beta, dcplx* C, int64_t ldc,
            int64_t strideC, int batch, bool allow_split) {
-  (void)allow_split;
-  zgemm_fp64(ctx, opA, opB, M, N, K, alpha, A, lda, strideA, B, ldb, strideB, beta, C, ldc, strideC, batch);
+  const bool split = ctx->precision == PREC_SPLIT_I8 && allow_split && ctx->force_fp64 == 0 && opA != OP_T &&
+                     opB != OP_T && alpha.imag() == 0.0 && (beta == cplx(0.0, 0.0) || beta == cplx(1.0, 0.0)) &&
+                     M >= 64 && N >= 64 && K >= 32 && (double)M * N * K >= 33554432.0;
+  if (!split) {
+    zgemm_fp64(ctx, opA, opB, M, N, K, alpha, A, lda, strideA, B, ldb, strideB, beta, C, ldc, strideC, batch);
+    return;
+  }
+  const int s = ctx->adaptive_slices ? slices_for_tol(ctx->split_tol) : ctx->nslices;
+  for (int b = 0; b < batch; ++b) {
+    const dcplx* Ab = A + strideA * b;
+    const dcplx* Bb = B + strideB * b;
+    auto SA = get_split(ctx, 0, opA, M, K, Ab, lda, s);
+    auto SB = get_split(ctx, 1, opB, N, K, Bb, ldb, s);
+    ctx->split_calls++;
+    split_gemm(ctx, *SA, *SB, s, alpha.real(), beta == cplx(1.0, 0.0), C + strideC * b, ldc);
+  }
 }
 
 }  // namespace imps

@@ -1,0 +1,113 @@
+"""The int8 split-precision complex GEMM (tcgen05) through the C ABI.
+
+* Integer-valued operands with |re|, |im| <= 100 are represented exactly by the
+  first slice, so the product must be bit-exact against the exact integer
+  product (this pins the MMA descriptors, the TMA layout and the epilogue).
+* Random operands: error bounded by the slice truncation, relative to |A||B|.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+import infinitempsalgorithms_b200 as imps
+from infinitempsalgorithms_b200 import _lib as L
+import oracle as O
+from gpu_helpers import rel, to_device_mpo, upload_envs, upload_state
+
+pytestmark = pytest.mark.gpu
+
+OPS = {"N": 0, "C": 2}
+
+
+def dev(a):
+    # column-major complex128 on the device: store the transpose row-major
+    return torch.from_numpy(np.ascontiguousarray(np.asarray(a, complex).T)).cuda()
+
+
+def host(t, shape):
+    return t.cpu().numpy().T.reshape(shape)
+
+
+def run_gemm(ctx, opA, opB, A, B, Cinit=None, beta=0.0):
+    Am = A if opA == "N" else A.conj().T
+    Bm = B if opB == "N" else B.conj().T
+    M, K = Am.shape
+    N = Bm.shape[1]
+    dA, dB = dev(A), dev(B)
+    Cd = dev(np.zeros((M, N), complex) if Cinit is None else Cinit)
+    st = ctx.lib.imps_zgemm(ctx.h, OPS[opA], OPS[opB], M, N, K, 1.0, 0.0, C.c_void_p(dA.data_ptr()), A.shape[0],
+                            C.c_void_p(dB.data_ptr()), B.shape[0], beta, 0.0, C.c_void_p(Cd.data_ptr()), M)
+    L.check(st, ctx.h)
+    return host(Cd, (M, N)), Am @ Bm
+
+
+@pytest.fixture()
+def split_ctx():
+    c = imps.Context(0)
+    c.set_precision(L.IMPS_PREC_SPLIT_I8, 2)
+    yield c
+    c.close()
+
+
+@pytest.mark.parametrize("M,N,K", [(64, 256, 64), (300, 520, 130), (128, 1000, 257)])
+@pytest.mark.parametrize("opA,opB", [("N", "N"), ("C", "N"), ("N", "C"), ("C", "C")])
+def test_split_gemm_bit_exact_integers(split_ctx, M, N, K, opA, opB):
+    rng = np.random.default_rng(M + N + K)
+    A0 = rng.integers(-100, 101, (M, K)) + 1j * rng.integers(-100, 101, (M, K))
+    B0 = rng.integers(-100, 101, (K, N)) + 1j * rng.integers(-100, 101, (K, N))
+    A = A0 if opA == "N" else A0.conj().T
+    B = B0 if opB == "N" else B0.conj().T
+    got, ref = run_gemm(split_ctx, opA, opB, A, B)
+    assert np.array_equal(got, ref), f"max diff {np.abs(got - ref).max()}"
+
+
+def test_split_gemm_accumulate(split_ctx):
+    rng = np.random.default_rng(7)
+    A = rng.integers(-50, 51, (200, 90)) + 1j * rng.integers(-50, 51, (200, 90))
+    B = rng.integers(-50, 51, (90, 300)) + 1j * rng.integers(-50, 51, (90, 300))
+    C0 = rng.integers(-9, 10, (200, 300)).astype(complex)
+    got, ref = run_gemm(split_ctx, "N", "N", A, B, Cinit=C0, beta=1.0)
+    assert np.array_equal(got, ref + C0)
+
+
+@pytest.mark.parametrize("s", [3, 4, 5, 6])
+def test_split_gemm_accuracy(s):
+    c = imps.Context(0)
+    c.set_precision(L.IMPS_PREC_SPLIT_I8, s)
+    rng = np.random.default_rng(s)
+    M, N, K = 384, 512, 640
+    A = rng.standard_normal((M, K)) + 1j * rng.standard_normal((M, K))
+    B = rng.standard_normal((K, N)) + 1j * rng.standard_normal((K, N))
+    A[:7] *= 1e-6  # rows of very different magnitude: per-row scaling must keep them accurate
+    got, ref = run_gemm(c, "N", "N", A, B)
+    # per element: truncation of each operand below 2^-7s of its row / column scale
+    # (scale < 2 x max(|re|, |im|)), summed over the 2K real products
+    ra = 2 * np.maximum(np.abs(A.real), np.abs(A.imag)).max(axis=1)
+    cb = 2 * np.maximum(np.abs(B.real), np.abs(B.imag)).max(axis=0)
+    bound = np.outer(ra, cb) * 2 * K * (s + 2) * 2.0 ** (-7 * s)
+    err = np.abs(got - ref)
+    assert np.all(err <= bound), f"worst ratio {np.max(err / bound)}"
+    c.close()
+
+
+def test_split_heff_matches_fp64():
+    # AC Heff through the split engine vs the FP64 engine on the same environments
+    c64 = imps.default_context()
+    cs = imps.Context(0)
+    cs.set_precision(L.IMPS_PREC_SPLIT_I8, 5)
+    oH = O.SchurMPO([O.hubbard_hamiltonian().Ws[0]])
+    opsi = O.randomimps([4], D=64, seed=3)
+    oenvs = O.build_envs(opsi, oH)
+    H = to_device_mpo(oH)
+    x = O.random_site_tensors([4], 64, 9)[0]
+    outs = []
+    for ctx in (c64, cs):
+        psi = upload_state(ctx, opsi)
+        envs = upload_envs(psi, H, oenvs)
+        outs.append(imps.AC_hamiltonian(1, psi, H, psi, envs)(x))
+    yref = O.ac_apply(oenvs.lefts[0], oH[0], oenvs.rights[0], x)
+    assert rel(outs[0], yref) < 1e-12
+    assert rel(outs[1], yref) < 1e-8
+    cs.close()
