@@ -12,6 +12,7 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+import weakref
 from dataclasses import dataclass, field
 from typing import Callable, List, Optional, Sequence
 
@@ -107,7 +108,13 @@ class Context:
         check(self.lib.imps_ctx_create(device, C.byref(h)))
         self.h = h
         self.device = device
+        self._children = weakref.WeakSet()
+        self._mpo_links = []
         self.set_precision(precision, nslices)
+
+    def _adopt(self, obj):
+        self._children.add(obj)
+        return obj
 
     def set_precision(self, mode: int, nslices: int = 5):
         check(self.lib.imps_ctx_set_precision(self.h, mode, nslices), self.h)
@@ -139,7 +146,11 @@ class Context:
         return dict(ac_apply=arr[0], c_apply=arr[1], push=arr[2], gemm=arr[3], kernels=arr[4])
 
     def close(self):
+        """Destroy the context; device objects created on it are released first."""
         if getattr(self, "h", None):
+            for child in list(self._children) + self._mpo_links:
+                child._release()
+            self._mpo_links = []
             self.lib.imps_ctx_destroy(self.h)
             self.h = None
 
@@ -219,14 +230,33 @@ class SparseIMPO:
             h = C.c_void_p()
             check(ctx.lib.imps_mpo_create(ctx.h, N, m, d, n, ptr_array(self.Ws), C.byref(h)), ctx.h)
             self._dev[key] = (ctx, h)
+            ctx._mpo_links.append(_MpoHandle(self, key))
         return self._dev[key][1]
 
+    def _release_key(self, key):
+        ent = self._dev.pop(key, None)
+        if ent is not None:
+            ent[0].lib.imps_mpo_destroy(ent[1])
+
     def __del__(self):
-        for ctx, h in getattr(self, "_dev", {}).values():
+        for key in list(getattr(self, "_dev", {})):
             try:
-                ctx.lib.imps_mpo_destroy(h)
+                self._release_key(key)
             except Exception:
                 pass
+
+
+class _MpoHandle:
+    """Weak link from a context to an MPO's device copy on it (released with the context)."""
+
+    def __init__(self, mpo, key):
+        self.mpo = weakref.ref(mpo)
+        self.key = key
+
+    def _release(self):
+        m = self.mpo()
+        if m is not None:
+            m._release_key(self.key)
 
 
 def tfim_hamiltonian(J=1.0, h=1.0) -> SparseIMPO:
@@ -296,6 +326,7 @@ class CanonicalIMPS:
         check(ctx.lib.imps_state_create(ctx.h, N, (C.c_int * N)(*self.dims), (C.c_int * N)(*self.chi), C.byref(h)),
               ctx.h)
         self.h = h
+        ctx._adopt(self)
 
     # constructors -----------------------------------------------------------
     @classmethod
@@ -383,11 +414,14 @@ class CanonicalIMPS:
         """``norm(psi) = norm(psi.AC[1])``."""
         return float(np.linalg.norm(self.get(L.IMPS_AC, 0)))
 
+    def _release(self):
+        if getattr(self, "h", None):
+            self.ctx.lib.imps_state_destroy(self.h)
+            self.h = None
+
     def __del__(self):
         try:
-            if getattr(self, "h", None):
-                self.ctx.lib.imps_state_destroy(self.h)
-                self.h = None
+            self._release()
         except Exception:
             pass
 
@@ -425,6 +459,7 @@ class DMRGCache:
         h = C.c_void_p()
         check(self.ctx.lib.imps_envs_create(self.ctx.h, psi.h, H.handle(self.ctx), C.byref(h)), self.ctx.h)
         self.h = h
+        self.ctx._adopt(self)
         self.N = len(psi)
         self.ml = [H[l + 1].shape[0] for l in range(self.N)]
         self.nr = [H[l + 1].shape[2] for l in range(self.N)]
@@ -471,11 +506,14 @@ class DMRGCache:
     def rights(self):
         return PeriodicVector(self.rightenv(l) for l in range(1, self.N + 1))
 
+    def _release(self):
+        if getattr(self, "h", None):
+            self.ctx.lib.imps_envs_destroy(self.h)
+            self.h = None
+
     def __del__(self):
         try:
-            if getattr(self, "h", None):
-                self.ctx.lib.imps_envs_destroy(self.h)
-                self.h = None
+            self._release()
         except Exception:
             pass
 

@@ -246,6 +246,7 @@ int imps_mpo_create(imps_ctx* h, int N, const int* m, const int* d, const int* n
   imps_mpo* mpo = new imps_mpo();
   int r = guard(&h->c, [&] {
     mpo->ctx = &h->c;
+    mpo->device = h->c.device;
     mpo->N = N;
     mpo->sites.resize(N);
     mpo->closing.resize(N);
@@ -268,10 +269,11 @@ int imps_mpo_create(imps_ctx* h, int N, const int* m, const int* d, const int* n
   return IMPS_OK;
 }
 
+// Destroy functions never dereference the context: an object may outlive it.
 int imps_mpo_destroy(imps_mpo* mpo) {
   if (!mpo) return IMPS_OK;
-  cudaSetDevice(mpo->ctx->device);
-  cudaStreamSynchronize(mpo->ctx->stream);
+  cudaSetDevice(mpo->device);
+  cudaDeviceSynchronize();
   delete mpo;
   return IMPS_OK;
 }
@@ -283,6 +285,7 @@ int imps_state_create(imps_ctx* h, int N, const int* d, const int* chi, imps_sta
   imps_state* st = new imps_state();
   int r = guard(&h->c, [&] {
     st->ctx = &h->c;
+    st->device = h->c.device;
     st->N = N;
     st->d.assign(d, d + N);
     st->chi.assign(chi, chi + N);
@@ -314,8 +317,8 @@ int imps_state_create(imps_ctx* h, int N, const int* d, const int* chi, imps_sta
 
 int imps_state_destroy(imps_state* st) {
   if (!st) return IMPS_OK;
-  cudaSetDevice(st->ctx->device);
-  cudaStreamSynchronize(st->ctx->stream);
+  cudaSetDevice(st->device);
+  cudaDeviceSynchronize();
   delete st;
   return IMPS_OK;
 }
@@ -422,6 +425,7 @@ int imps_envs_create(imps_ctx* h, const imps_state* st, const imps_mpo* mpo, imp
   imps_envs* E = new imps_envs();
   int r = guard(&h->c, [&] {
     E->ctx = &h->c;
+    E->device = h->c.device;
     imps::envs_allocate(E, st, mpo);
     for (int l = 0; l < E->N; ++l) {
       imps::zfill(&h->c, (int64_t)(E->lefts[l].bytes / sizeof(imps::dcplx)), 0.0, E->lefts[l].z());
@@ -439,8 +443,8 @@ int imps_envs_create(imps_ctx* h, const imps_state* st, const imps_mpo* mpo, imp
 
 int imps_envs_destroy(imps_envs* E) {
   if (!E) return IMPS_OK;
-  cudaSetDevice(E->ctx->device);
-  cudaStreamSynchronize(E->ctx->stream);
+  cudaSetDevice(E->device);
+  cudaDeviceSynchronize();
   delete E;
   return IMPS_OK;
 }

@@ -203,6 +203,7 @@ struct MpoSite {
 
 struct imps_mpo {
   imps::Context* ctx;
+  int device = 0;
   int N;
   std::vector<imps::MpoSite> sites;
   std::vector<imps::MpoSite> closing;  // closing column (m, d, 1, d) of each site, for the Schur energy
@@ -212,6 +213,7 @@ struct imps_mpo {
 
 struct imps_state {
   imps::Context* ctx;
+  int device = 0;
   int N;
   std::vector<int> d;     // physical dim per site
   std::vector<int> chi;   // chi[l] = bond dimension right of site l (bond N-1 == bond 0)
@@ -224,6 +226,7 @@ struct imps_state {
 
 struct imps_envs {
   imps::Context* ctx;
+  int device = 0;
   int N;
   std::vector<int> Dl, Dr, ml, nr;
   std::vector<imps::DevBuf> lefts, rights;   // (Dl, ml, Dl), (Dr, nr, Dr)

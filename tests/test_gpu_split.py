@@ -98,10 +98,10 @@ def test_split_heff_matches_fp64():
     cs = imps.Context(0)
     cs.set_precision(L.IMPS_PREC_SPLIT_I8, 5)
     oH = O.SchurMPO([O.hubbard_hamiltonian().Ws[0]])
-    opsi = O.randomimps([4], D=64, seed=3)
+    opsi = O.randomimps([4], D=128, seed=3)
     oenvs = O.build_envs(opsi, oH)
     H = to_device_mpo(oH)
-    x = O.random_site_tensors([4], 64, 9)[0]
+    x = O.random_site_tensors([4], 128, 9)[0]
     outs = []
     for ctx in (c64, cs):
         psi = upload_state(ctx, opsi)
