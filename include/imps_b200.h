@@ -161,6 +161,19 @@ int imps_envs_set(imps_envs* envs, int side, int site, const double* host);
 /* MPO_AC_Hamiltonian action (src/algorithms/groundstates/effective.jl:66-68, 90-102). */
 int imps_ac_apply(imps_envs* envs, const imps_mpo* mpo, int site, const double* x, double* y);
 int imps_ac_apply_dev(imps_envs* envs, const imps_mpo* mpo, int site, const void* x_dev, void* y_dev);
+/* Allocation-free AC apply -- no counterpart in the reference.  For callers that
+ * cannot let the library call cudaMalloc (their caching allocator already holds
+ * the device memory, or they must avoid the implicit synchronisation of
+ * cudaMalloc/cudaFree): the same FP64 GL.x -> level mix -> .GR pipeline as
+ * imps_ac_apply, every intermediate held in one fixed 64 MiB device array of the
+ * library (per device, kept until exit).  GL (Dl, m, Dl), GR (Dr, n, Dr), x, y
+ * (Dl, d, Dr) are caller-owned device buffers, W_host the (m, d, n, d) MPO tensor
+ * in host memory (<= 64 KiB).  Sizes needing more than the array
+ * (16*Dl*d*Dr*(m+n) bytes) return IMPS_INVALID_ARG.  All calls share the array:
+ * calls whose GPU work overlaps race.  The first call on a device looks up the
+ * array's address; make it before any stream capture. */
+int imps_ac_apply_noalloc(imps_ctx* ctx, int Dl, int d, int Dr, int m, int n, const double* W_host,
+                          const void* GL_dev, const void* GR_dev, const void* x_dev, void* y_dev);
 /* MPO_C_Hamiltonian action (effective.jl:52-54, 72-76): GL = lefts[site+1], GR = rights[site]. */
 int imps_c_apply(imps_envs* envs, int site, const double* x, double* y);
 int imps_c_apply_dev(imps_envs* envs, int site, const void* x_dev, void* y_dev);

@@ -102,6 +102,7 @@ _SIGS = {
     "imps_envs_set": (I32, [P, I32, I32, DP]),
     "imps_ac_apply": (I32, [P, P, I32, DP, DP]),
     "imps_ac_apply_dev": (I32, [P, P, I32, P, P]),
+    "imps_ac_apply_noalloc": (I32, [P, I32, I32, I32, I32, I32, DP, P, P, P, P]),
     "imps_c_apply": (I32, [P, I32, DP, DP]),
     "imps_c_apply_dev": (I32, [P, I32, P, P]),
     "imps_push_left": (I32, [P, I32, I32, I32, DP, DP, DP, DP]),

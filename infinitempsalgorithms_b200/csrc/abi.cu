@@ -508,6 +508,17 @@ int imps_ac_apply(imps_envs* E, const imps_mpo* mpo, int site, const double* x, 
   });
 }
 
+int imps_ac_apply_noalloc(imps_ctx* h, int Dl, int d, int Dr, int m, int n, const double* W_host, const void* GL,
+                          const void* GR, const void* x, void* y) {
+  if (!h || !W_host || !GL || !GR || !x || !y) return IMPS_INVALID_ARG;
+  return guard(&h->c, [&] {
+    imps::ac_apply_noalloc(&h->c, Dl, d, Dr, m, n, hc(W_host), static_cast<const imps::dcplx*>(GL),
+                           static_cast<const imps::dcplx*>(GR), static_cast<const imps::dcplx*>(x),
+                           static_cast<imps::dcplx*>(y));
+    return IMPS_OK;
+  });
+}
+
 int imps_c_apply_dev(imps_envs* E, int site, const void* x, void* y) {
   if (!E || !x || !y) return IMPS_INVALID_ARG;
   return guard(E->ctx, [&] {

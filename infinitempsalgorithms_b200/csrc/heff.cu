@@ -79,20 +79,27 @@ __global__ void k_scale_cols_rows(int m, int n, int k, dcplx* Q, int64_t ldq, dc
 
 }  // namespace
 
-void level_mix(Context* ctx, const MixPlan& plan, const dcplx* in, dcplx* out) {
+void level_mix_nz(Context* ctx, const MixPlan& plan, const std::pair<int, int>* nz_in, int nnz, const dcplx* in,
+                  dcplx* out) {
   MixArgs a;
   a.Db = plan.Db; a.R = plan.R; a.P = plan.P; a.Q = plan.Q; a.S = plan.S; a.Cn = plan.C;
   a.in_r = plan.in_r; a.in_s = plan.in_s; a.in_c = plan.in_c;
   a.out_p = plan.out_p; a.out_q = plan.out_q; a.out_c = plan.out_c;
   a.scale = make_double2(plan.scale.real(), plan.scale.imag());
-  // group the nonzero (r, q) blocks by q
-  std::vector<std::pair<int, int>> nz(plan.nz);
-  std::sort(nz.begin(), nz.end(), [](const std::pair<int, int>& x, const std::pair<int, int>& y) {
-    return x.second != y.second ? x.second < y.second : x.first < y.first;
-  });
-  IMPS_REQUIRE((int)nz.size() <= kMaxNz, IMPS_INVALID_ARG, "level_mix: too many MPO blocks");
+  IMPS_REQUIRE(nnz <= kMaxNz, IMPS_INVALID_ARG, "level_mix: too many MPO blocks");
+  // group the nonzero (r, q) blocks by q (insertion sort into a fixed array: no heap use)
+  std::pair<int, int> nz[kMaxNz];
+  for (int t = 0; t < nnz; ++t) {
+    std::pair<int, int> v = nz_in[t];
+    int u = t;
+    while (u > 0 && (nz[u - 1].second > v.second || (nz[u - 1].second == v.second && nz[u - 1].first > v.first))) {
+      nz[u] = nz[u - 1];
+      --u;
+    }
+    nz[u] = v;
+  }
   a.nq = 0;
-  for (size_t t = 0; t < nz.size(); ++t) {
+  for (int t = 0; t < nnz; ++t) {
     if (a.nq == 0 || a.qval[a.nq - 1] != nz[t].second) {
       IMPS_REQUIRE(a.nq < kMaxQ, IMPS_INVALID_ARG, "level_mix: too many MPO levels");
       a.qval[a.nq] = (short)nz[t].second;
@@ -101,7 +108,7 @@ void level_mix(Context* ctx, const MixPlan& plan, const dcplx* in, dcplx* out) {
     }
     a.rval[t] = (short)nz[t].first;
   }
-  a.qstart[a.nq] = (short)nz.size();
+  a.qstart[a.nq] = (short)nnz;
   if (a.nq == 0 || plan.Db <= 0 || plan.C <= 0) return;
   dim3 block(128);
   dim3 grid((plan.Db + 127) / 128, std::min(plan.C, 65535));
@@ -118,6 +125,10 @@ void level_mix(Context* ctx, const MixPlan& plan, const dcplx* in, dcplx* out) {
   ctx->n_kernels++;
   cudaError_t e = cudaPeekAtLastError();
   if (e != cudaSuccess) throw Error(IMPS_CUDA_ERROR, std::string("level_mix launch: ") + cudaGetErrorString(e));
+}
+
+void level_mix(Context* ctx, const MixPlan& plan, const dcplx* in, dcplx* out) {
+  level_mix_nz(ctx, plan, plan.nz.data(), (int)plan.nz.size(), in, out);
 }
 
 // Phase fix shared by qrpos/lqpos (see linalg.cu)

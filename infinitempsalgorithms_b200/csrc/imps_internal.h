@@ -269,6 +269,9 @@ struct MixPlan {
   cplx scale = cplx(1.0, 0.0);
 };
 void level_mix(Context* ctx, const MixPlan& plan, const dcplx* in, dcplx* out);
+// same with the block list given as a pointer (uses no heap memory; plan.nz is ignored)
+void level_mix_nz(Context* ctx, const MixPlan& plan, const std::pair<int, int>* nz, int nnz, const dcplx* in,
+                  dcplx* out);
 
 // BLAS-1 style helpers (deterministic two-pass reductions)
 void zcopy(Context* ctx, int64_t n, const dcplx* x, dcplx* y);
@@ -326,6 +329,10 @@ void push_right_levels(Context* ctx, const MpoSite& W, int Dl, int d, int Dr, co
                        int64_t R_level_stride, int64_t R_ld, const std::vector<std::pair<int, int>>& blocks,
                        const std::vector<int>& q_targets, const dcplx* A, dcplx* out, int64_t out_level_stride,
                        int64_t out_ld, bool accumulate);
+// AC apply with all intermediates in a fixed file-scope device array (noalloc.cu)
+void ac_apply_noalloc(Context* ctx, int Dl, int d, int Dr, int m, int n, const cplx* W_host, const dcplx* GL,
+                      const dcplx* GR, const dcplx* x, dcplx* y);
+size_t noalloc_scratch_bytes();
 // Full MPO pushes (transfer_leftenv!/transfer_rightenv!)
 void push_mpo_left(Context* ctx, const MpoSite& W, int Dl, int d, int Dr, const dcplx* L, const dcplx* A, dcplx* out);
 void push_mpo_right(Context* ctx, const MpoSite& W, int Dl, int d, int Dr, const dcplx* R, const dcplx* A,
