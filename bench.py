@@ -44,8 +44,10 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--precision", default="fp64", choices=["fp64", "split"])
-    p.add_argument("--nslices", type=int, default=5)
+    p.add_argument("--nslices", type=int, default=0, help="int8 slices (0 = adaptive to the solver tolerance)")
     p.add_argument("--D", type=int, default=WORKLOAD["D"])
+    p.add_argument("--mode", default="vumps", choices=["vumps", "heff"],
+                   help="vumps: one VUMPS iteration per step; heff: one AC Heff apply per step")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     return p.parse_args()
@@ -253,6 +255,57 @@ def run_ours(args, world, rank, local):
     return result, ctx, psi, envs, H
 
 
+def run_heff(args, world, rank, local):
+    """AC effective-Hamiltonian matvecs/s at the workload's D (site 1, random
+    environments of the right shape): the dominant operation of every solver."""
+    import torch
+    import ctypes as C
+    import infinitempsalgorithms_b200 as imps
+    from infinitempsalgorithms_b200 import _lib as L
+    torch.cuda.set_device(local)
+    ctx = imps.Context(local)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    if args.precision == "split":
+        ctx.set_precision(L.IMPS_PREC_SPLIT_I8, args.nslices if args.nslices > 0 else 5)
+    D = args.D
+    H = imps.hubbard_hamiltonian()
+    d, w = 4, 6
+    psi = imps.CanonicalIMPS(ctx, [d], [D])
+    envs = imps.DMRGCache(psi, H, build=False)
+    rng = np.random.default_rng(rank)
+    envs.set_leftenv(1, rng.standard_normal((D, w, D)) + 1j * rng.standard_normal((D, w, D)))
+    envs.set_rightenv(1, rng.standard_normal((D, w, D)) + 1j * rng.standard_normal((D, w, D)))
+    x = torch.randn(D * d * D, dtype=torch.complex128, device="cuda")
+    y = torch.zeros_like(x)
+    Hh = H.handle(ctx)
+
+    def apply():
+        L.check(ctx.lib.imps_ac_apply_dev(envs.h, Hh, 0, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr())), ctx.h)
+    for _ in range(args.warmup):
+        apply()
+    torch.cuda.synchronize()
+    barrier(world)
+    ctx.profile(True)
+    ctx.profile_reset()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        apply()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = allmax(world, e0.elapsed_time(e1))
+    prof = {k: ctx.profile_get(k) for k in ("zgemm_fp64", "gemm_split", "level_mix", "split_slice")}
+    return {"metric": f"AC Heff matvecs/s (Hubbard JW, D={D})", "value": args.steps * world / (ms / 1e3),
+            "unit": "matvec/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "tflops_alg": ac_flops(D, d, w) * args.steps / (ms / 1e3) / 1e12,
+            "config": {"workload": "ac_heff_hubbard_jw", "D": D, "precision": args.precision,
+                       "nslices": args.nslices if args.precision == "split" else None},
+            "kernel_ms": {k: round(v[1] / args.steps, 3) for k, v in prof.items()}}
+
+
 def run_e2e(args, ctx, psi, envs, H, it, eps, world):
     """Same metric through the C ABI with host buffers: each step uploads the
     state (AL/AR/C/AC of both sites) from pinned host memory, runs
@@ -362,6 +415,11 @@ def main():
     world, rank, local = dist_init(args)
     if args.impl == "reference":
         res = run_reference(args, world, rank)
+        if rank == 0:
+            print(json.dumps(res))
+        return
+    if args.mode == "heff":
+        res = run_heff(args, world, rank, local)
         if rank == 0:
             print(json.dumps(res))
         return

@@ -26,6 +26,7 @@ double dyn_tol(double eps, double factor, int iter) {
 }  // namespace
 
 double galerkin(Context* ctx, imps_envs* E, const imps_mpo* H, const imps_state* st) {
+  Fp64Scope fp64(ctx);  // the Galerkin residual is always FP64
   double eps = 0.0;
   for (int site = 0; site < st->N; ++site) {
     const int Dl = st->Dl(site), d = st->d[site], Dr = st->Dr(site);
@@ -45,6 +46,7 @@ double galerkin(Context* ctx, imps_envs* E, const imps_mpo* H, const imps_state*
 }
 
 cplx energy(Context* ctx, imps_envs* E, const imps_mpo* H, imps_state* st) {
+  Fp64Scope fp64(ctx);
   cplx e = 0.0;
   for (int site = 0; site < st->N; ++site) {
     const MpoSite& col = H->closing[site % H->N];
@@ -60,6 +62,7 @@ cplx energy(Context* ctx, imps_envs* E, const imps_mpo* H, imps_state* st) {
 }
 
 cplx local_expval(Context* ctx, imps_state* st, int site, const cplx* O) {
+  Fp64Scope fp64(ctx);
   const int Dl = st->Dl(site), d = st->d[site], Dr = st->Dr(site);
   const int64_t n = (int64_t)Dl * d * Dr;
   DevBuf& y = ctx->buf("lexp_y", n * sizeof(dcplx));
@@ -77,23 +80,59 @@ cplx local_expval(Context* ctx, imps_state* st, int site, const cplx* O) {
   return v / state_dot(ctx, st);
 }
 
+namespace {
+// Lanczos on the split engine, then (if the engine's accuracy floor is above the
+// requested tolerance) an FP64 Lanczos polish warm-started from the split result.
+// `hest` is a running estimate of |lambda|, the scale of the matvec error.
+KrylovResult mixed_eigsolve(Context* ctx, int64_t n, const LinOp& op, const dcplx* x0, dcplx* x, double tol, int kdim,
+                            int maxiter, bool eager, double& hest) {
+  if (ctx->precision != PREC_SPLIT_I8 || ctx->force_fp64 > 0)
+    return lanczos_eigsolve(ctx, n, op, x0, x, tol, kdim, maxiter, eager);
+  const double scale = hest > 0 ? hest : 1.0;
+  KrylovResult r1;
+  double floor_abs;
+  {
+    TolScope ts(ctx, tol / (8.0 * scale));
+    floor_abs = split_floor(ctx) * scale;
+    r1 = lanczos_eigsolve(ctx, n, op, x0, x, std::max(tol, floor_abs), kdim, maxiter, eager);
+  }
+  hest = std::max(std::abs(r1.value), 1e-300);
+  if (floor_abs <= tol) return r1;
+  KrylovResult r2;
+  {
+    Fp64Scope fp64(ctx);
+    r2 = lanczos_eigsolve(ctx, n, op, x, x, tol, kdim, maxiter, eager);
+  }
+  r2.numops += r1.numops;
+  r2.numiter += r1.numiter;
+  return r2;
+}
+}  // namespace
+
 KrylovResult eigsolve_ac(Context* ctx, imps_envs* E, const imps_mpo* H, int site, const dcplx* x0, dcplx* x,
                          double tol, int kdim, int maxiter, bool eager) {
   const int64_t n = (int64_t)E->Dl[site] * H->sites[site % H->N].d * E->Dr[site];
+  ConstScope cs(ctx, {E->lefts[site].ptr, E->rights[site].ptr});
   LinOp op = [&](const dcplx* v, dcplx* out) { ac_apply(ctx, E, H, site, v, out); };
-  return lanczos_eigsolve(ctx, n, op, x0, x, tol, kdim, maxiter, eager);
+  return mixed_eigsolve(ctx, n, op, x0, x, tol, kdim, maxiter, eager, E->hest_ac[site]);
 }
 
 KrylovResult eigsolve_c(Context* ctx, imps_envs* E, int site, const dcplx* x0, dcplx* x, double tol, int kdim,
                         int maxiter, bool eager) {
   const int64_t n = (int64_t)E->Dr[site] * E->Dr[site];
+  const int l1 = (site + 1) % E->N;
+  ensure_GLp(ctx, E, l1);
+  ConstScope cs(ctx, {E->GLp[l1].ptr, E->rights[site].ptr});
   LinOp op = [&](const dcplx* v, dcplx* out) { c_apply(ctx, E, site, v, out); };
-  return lanczos_eigsolve(ctx, n, op, x0, x, tol, kdim, maxiter, eager);
+  return mixed_eigsolve(ctx, n, op, x0, x, tol, kdim, maxiter, eager, E->hest_c[site]);
 }
 
 KrylovResult expo_ac(Context* ctx, imps_envs* E, const imps_mpo* H, int site, cplx dt, const dcplx* x0, dcplx* x,
                      double tol, int kdim, int maxiter) {
   const int64_t n = (int64_t)E->Dl[site] * H->sites[site % H->N].d * E->Dr[site];
+  ConstScope cs(ctx, {E->lefts[site].ptr, E->rights[site].ptr});
+  const double scale = (E->hest_ac[site] > 0 ? E->hest_ac[site] : 1.0) * std::max(std::abs(dt), 1e-300);
+  TolScope ts(ctx, tol / (8.0 * scale));
   LinOp op = [&](const dcplx* v, dcplx* out) { ac_apply(ctx, E, H, site, v, out); };
   return exponentiate(ctx, n, op, dt, x0, x, tol, kdim, maxiter);
 }
@@ -101,6 +140,11 @@ KrylovResult expo_ac(Context* ctx, imps_envs* E, const imps_mpo* H, int site, cp
 KrylovResult expo_c(Context* ctx, imps_envs* E, int site, cplx dt, const dcplx* x0, dcplx* x, double tol, int kdim,
                     int maxiter) {
   const int64_t n = (int64_t)E->Dr[site] * E->Dr[site];
+  const int l1 = (site + 1) % E->N;
+  ensure_GLp(ctx, E, l1);
+  ConstScope cs(ctx, {E->GLp[l1].ptr, E->rights[site].ptr});
+  const double scale = (E->hest_c[site] > 0 ? E->hest_c[site] : 1.0) * std::max(std::abs(dt), 1e-300);
+  TolScope ts(ctx, tol / (8.0 * scale));
   LinOp op = [&](const dcplx* v, dcplx* out) { c_apply(ctx, E, site, v, out); };
   return exponentiate(ctx, n, op, dt, x0, x, tol, kdim, maxiter);
 }

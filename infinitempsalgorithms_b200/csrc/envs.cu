@@ -101,6 +101,8 @@ struct Builder {
 
   // x <- solution of (1 - op) x = rhs with GMRES (linsolve with a0 = 1, a1 = -1)
   void solve(const LinOp& op, int D, Slice target, const dcplx* prev_contig) {
+    // GMRES refines in FP64, so the inner Krylov cycles only need a moderate accuracy
+    TolScope inner(ctx, 1e-6);
     const int64_t n = (int64_t)D * D;
     DevBuf& rhs = ctx->buf("env_rhs", n * sizeof(dcplx));
     DevBuf& x = ctx->buf("env_x", n * sizeof(dcplx));
@@ -140,6 +142,8 @@ struct Builder {
   void run() {
     const int N = this->N();
     info.converged = 1;
+    // right-hand-side sweeps: error of the split engine kept well below the solver tolerance
+    TolScope rhs_tol(ctx, tol * 1e-2);
     const int DN = st->Dr(N - 1);
     // rho_r = C[N] C[N]^H (left solves), rho_l = C[N]^H C[N] (right solves)
     DevBuf& rho_r = ctx->buf("env_rho_r", (size_t)DN * DN * sizeof(dcplx));
@@ -324,6 +328,8 @@ void envs_allocate(imps_envs* E, const imps_state* st, const imps_mpo* H) {
   E->init_rights.resize(N);
   E->GLp.resize(N);
   E->GLp_valid.assign(N, false);
+  E->hest_ac.assign(N, 0.0);
+  E->hest_c.assign(N, 0.0);
   for (int l = 0; l < N; ++l) {
     const MpoSite& W = H->sites[l % H->N];
     IMPS_REQUIRE(W.d == st->d[l], IMPS_DIM_MISMATCH, "MPO physical dimension != state physical dimension");
@@ -362,6 +368,13 @@ imps_env_info envs_build(Context* ctx, imps_envs* E, const imps_state* st, const
     zset_identity(ctx, Dr, r.p, r.ld, 1.0);
     E->GLp_valid[l] = false;
   }
+  // the site tensors are constant for the whole build: their int8 splits are cached
+  std::vector<const void*> cptrs;
+  for (int l = 0; l < N; ++l) {
+    cptrs.push_back(st->AL[l].ptr);
+    cptrs.push_back(st->AR[l].ptr);
+  }
+  ConstScope cs(ctx, cptrs);
   Builder b;
   b.ctx = ctx;
   b.E = E;

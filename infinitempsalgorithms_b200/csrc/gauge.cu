@@ -46,6 +46,7 @@ double diff_norm(Context* ctx, int64_t n, const dcplx* a, const dcplx* b) {
 
 GaugeResult uniform_leftorth(Context* ctx, imps_state* st, const std::vector<const dcplx*>& A, const dcplx* C0,
                              double tol, int maxiter, int eig_miniter) {
+  Fp64Scope fp64(ctx);  // gauge fixing stays FP64
   const int N = st->N;
   GaugeResult res;
   std::vector<dcplx*> Aw = work_copy(ctx, st, A, "gauge_awork");
@@ -104,6 +105,7 @@ GaugeResult uniform_leftorth(Context* ctx, imps_state* st, const std::vector<con
 
 GaugeResult uniform_rightorth(Context* ctx, imps_state* st, const std::vector<const dcplx*>& A, const dcplx* C0,
                               double tol, int maxiter, int eig_miniter) {
+  Fp64Scope fp64(ctx);
   const int N = st->N;
   GaugeResult res;
   std::vector<dcplx*> Aw = work_copy(ctx, st, A, "gauge_awork");
@@ -208,6 +210,7 @@ GaugeResult from_al(Context* ctx, imps_state* st, const dcplx* C0, double tol, i
 }
 
 void regauge(Context* ctx, int Dl, int d, int Dr, const dcplx* AC, const dcplx* C, dcplx* AL) {
+  Fp64Scope fp64(ctx);
   DevBuf& Qac = ctx->buf("reg_qac", (size_t)Dl * d * Dr * sizeof(dcplx));
   DevBuf& Rac = ctx->buf("reg_rac", (size_t)Dr * Dr * sizeof(dcplx));
   DevBuf& Qc = ctx->buf("reg_qc", (size_t)Dr * Dr * sizeof(dcplx));
@@ -219,6 +222,7 @@ void regauge(Context* ctx, int Dl, int d, int Dr, const dcplx* AC, const dcplx* 
 }
 
 cplx state_dot(Context* ctx, imps_state* st) {
+  Fp64Scope fp64(ctx);
   const int N = st->N, D0 = st->Dl(0);
   DevBuf& v0 = ctx->buf("dot_v0", (size_t)D0 * D0 * sizeof(dcplx));
   DevBuf& ev = ctx->buf("dot_ev", (size_t)D0 * D0 * sizeof(dcplx));

@@ -175,7 +175,7 @@ void ac_apply(Context* ctx, const imps_envs* envs, const imps_mpo* mpo, int site
         (int64_t)Dl * d, 0, 1);
 }
 
-static void ensure_GLp(Context* ctx, imps_envs* envs, int l) {
+void ensure_GLp(Context* ctx, imps_envs* envs, int l) {
   if (envs->GLp_valid[l]) return;
   const int D = envs->Dl[l], w = envs->ml[l];
   envs->GLp[l].ensure((size_t)D * D * w * sizeof(dcplx));

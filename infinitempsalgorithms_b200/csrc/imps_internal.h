@@ -176,6 +176,12 @@ struct TolScope {
   ~TolScope() { ctx->split_tol = old; }
 };
 
+// Slices the split engine would use right now (0 = FP64 engine).  Adaptive mode picks
+// the smallest s whose truncation floor meets ctx->split_tol; s >= 7 falls back to FP64.
+int active_slices(const Context* ctx);
+// Relative accuracy of the GEMM engine currently selected (0 for FP64).
+double split_floor(const Context* ctx);
+
 // RAII timer for one kernel class on the context stream (active when profiling).
 struct ScopedTimer {
   Context* ctx;
@@ -238,6 +244,8 @@ struct imps_envs {
   std::vector<bool> GLp_valid;
   int64_t version = 0;
   imps_env_info last;
+  // operator-scale estimates |lambda| of the AC / C problems (split-precision accuracy targets)
+  std::vector<double> hest_ac, hest_c;
 };
 
 namespace imps {
@@ -315,6 +323,8 @@ void download(Context* ctx, void* dst, const void* src, size_t bytes);
 void ac_apply(Context* ctx, const imps_envs* envs, const imps_mpo* mpo, int site, const dcplx* x, dcplx* y,
               const MpoSite* Wover = nullptr, const dcplx* GRover = nullptr, int64_t GRover_ld = 0);
 void c_apply(Context* ctx, imps_envs* envs, int site, const dcplx* x, dcplx* y);
+// (re)build the permuted left environment GLp[l] used by c_apply
+void ensure_GLp(Context* ctx, imps_envs* envs, int l);
 // identity-channel pushes with distinct above/below tensors (transfermatrix.jl:5-66)
 void push_left_id(Context* ctx, int Dl, int d, int Dr, const dcplx* L, const dcplx* above, const dcplx* below,
                   dcplx* out);

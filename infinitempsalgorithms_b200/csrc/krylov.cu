@@ -138,8 +138,17 @@ KrylovResult gmres(Context* ctx, int64_t n, const LinOp& A, const dcplx* b, dcpl
     A(v, out);
     zaxpby(ctx, n, a0, v, a1, out);  // out = a0 v + a1 A v
   };
+  // Mixed precision = iterative refinement: the residual b - op(x) that defines
+  // convergence is always evaluated with the FP64 engine; the Krylov cycles in
+  // between run on the split engine and solve the correction equation to the
+  // engine's relative accuracy.
+  const double inner_floor = split_floor(ctx);
+  auto true_op = [&](const dcplx* v, dcplx* out) {
+    Fp64Scope f(ctx);
+    op(v, out);
+  };
   // r = b - op(x)
-  op(x, V);
+  true_op(x, V);
   zaxpby(ctx, n, 1.0, b, -1.0, V);
   double beta = dznrm2(ctx, n, V);
   res.normres = beta;
@@ -180,7 +189,7 @@ KrylovResult gmres(Context* ctx, int64_t n, const LinOp& A, const dcplx* b, dcpl
       g[k] = cs[k] * g[k];
       for (int i = 0; i <= k + 1; ++i) R[i + (size_t)ldr * k] = col[i];
       kused = k + 1;
-      if (std::abs(g[k + 1]) <= tol || hn <= 1e-300) break;
+      if (std::abs(g[k + 1]) <= std::max(tol, inner_floor * beta) || hn <= 1e-300) break;
       zscal(ctx, n, 1.0 / hn, w);
     }
     std::vector<cplx> y(kused, 0.0);
@@ -190,7 +199,7 @@ KrylovResult gmres(Context* ctx, int64_t n, const LinOp& A, const dcplx* b, dcpl
       y[i] = s / R[i + (size_t)ldr * i];
     }
     zgemv_acc(ctx, n, kused, V, n, y.data(), x);
-    op(x, V);
+    true_op(x, V);
     zaxpby(ctx, n, 1.0, b, -1.0, V);
     beta = dznrm2(ctx, n, V);
     res.normres = beta;

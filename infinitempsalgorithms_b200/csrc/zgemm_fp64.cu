@@ -177,11 +177,22 @@ void zgemm_fp64(Context* ctx, Op opA, Op opB, int M, int N, int K, cplx alpha, c
 }
 
 int slices_for_tol(double tol) {
-  // truncation error of s slices is below 2^-7s of the row/column scale; keep a
-  // 2^6 margin for the K-sum and the operator norm
+  // the truncation error of s slices is below 2^-7s of the row/column scales; keep
+  // a 2^4 margin for the sum over K and the spread inside a row
   if (!(tol > 0)) return 7;
-  int s = (int)std::ceil((-std::log2(tol) + 6.0) / 7.0);
+  int s = (int)std::ceil((-std::log2(tol) + 4.0) / 7.0);
   return std::min(7, std::max(2, s));
+}
+
+int active_slices(const Context* ctx) {
+  if (ctx->precision != PREC_SPLIT_I8 || ctx->force_fp64 > 0) return 0;
+  const int s = ctx->adaptive_slices ? slices_for_tol(ctx->split_tol) : ctx->nslices;
+  return s >= 7 ? 0 : s;  // seven slices cost about as much as the FP64 engine
+}
+
+double split_floor(const Context* ctx) {
+  const int s = active_slices(ctx);
+  return s == 0 ? 0.0 : 16.0 * std::ldexp(1.0, -7 * s);
 }
 
 static std::shared_ptr<SplitOperand> get_split(Context* ctx, int side, Op op, int rows, int K, const dcplx* X,
@@ -212,14 +223,14 @@ static std::shared_ptr<SplitOperand> get_split(Context* ctx, int side, Op op, in
 void zgemm(Context* ctx, Op opA, Op opB, int M, int N, int K, cplx alpha, const dcplx* A, int64_t lda,
            int64_t strideA, const dcplx* B, int64_t ldb, int64_t strideB, cplx beta, dcplx* C, int64_t ldc,
            int64_t strideC, int batch, bool allow_split) {
-  const bool split = ctx->precision == PREC_SPLIT_I8 && allow_split && ctx->force_fp64 == 0 && opA != OP_T &&
-                     opB != OP_T && alpha.imag() == 0.0 && (beta == cplx(0.0, 0.0) || beta == cplx(1.0, 0.0)) &&
-                     M >= 64 && N >= 64 && K >= 32 && (double)M * N * K >= 33554432.0;
+  const int s = active_slices(ctx);
+  const bool split = s > 0 && allow_split && opA != OP_T && opB != OP_T && alpha.imag() == 0.0 &&
+                     (beta == cplx(0.0, 0.0) || beta == cplx(1.0, 0.0)) && M >= 64 && N >= 64 && K >= 32 &&
+                     (double)M * N * K >= 33554432.0;
   if (!split) {
     zgemm_fp64(ctx, opA, opB, M, N, K, alpha, A, lda, strideA, B, ldb, strideB, beta, C, ldc, strideC, batch);
     return;
   }
-  const int s = ctx->adaptive_slices ? slices_for_tol(ctx->split_tol) : ctx->nslices;
   for (int b = 0; b < batch; ++b) {
     const dcplx* Ab = A + strideA * b;
     const dcplx* Bb = B + strideB * b;
