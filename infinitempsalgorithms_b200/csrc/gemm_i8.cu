@@ -33,14 +33,16 @@ namespace imps {
 namespace {
 
 constexpr int BM = 128;          // tile rows (real rows of At)
-constexpr int BN = 256;          // tile cols (rows of Bt)
+constexpr int BN = 128;          // tile cols (rows of Bt)
 constexpr int BKB = 128;         // K bytes per stage (one 128B swizzle atom)
-constexpr int STAGES = 4;
+constexpr int STAGES = 6;
+constexpr int NSLOT = 4;         // TMEM accumulator slots of BN columns (4 x 128 = 512)
+constexpr int EPI_WARPS = 8;     // two warps per TMEM lane quarter, each owning BN/2 columns
 constexpr int A_STAGE = BM * BKB;   // 16 KB
 constexpr int B_STAGE = BN * BKB;   // 32 KB
 constexpr int SMEM_TILES = STAGES * (A_STAGE + B_STAGE);
 constexpr int SMEM_BYTES = SMEM_TILES + 1024 /*align*/ + 256 /*barriers*/;
-constexpr int NTHREADS = 192;
+constexpr int NTHREADS = 32 * (2 + EPI_WARPS);
 constexpr long long WAIT_CYCLES = 2000000000LL;   // ~1 s at 1.9 GHz
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -65,10 +67,15 @@ __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// bounded wait: returns false (and raises the error flag) after ~1 s
+// bounded wait: returns false (and raises the error flag) after ~1 s.  The fast path
+// only polls the barrier; the global error flag and the clock are checked every
+// 256 unsuccessful polls so a completed phase is seen without extra memory latency.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* err) {
-  long long t0 = clock64();
+  if (mbar_try(bar, parity)) return true;
+  const long long t0 = clock64();
+  unsigned spins = 0;
   while (!mbar_try(bar, parity)) {
+    if ((++spins & 255u) != 0u) continue;
     if (*err) return false;
     if (clock64() - t0 > WAIT_CYCLES) {
       atomicExch((int*)err, 1);
@@ -132,18 +139,38 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, int32_t* r) {
 
 struct GemmArgs {
   int num_m, num_n;          // tiles
+  int n_fast;                // raster: 1 -> consecutive tiles walk N (A is the larger operand)
   int kblocks;               // K blocks of 128 bytes per slice plane
-  int diag;                  // slice diagonal d
-  int kb_begin, kb_end;      // K-chunk [kb_begin, kb_end) within each plane
+  int s;                     // slice diagonals d = 0 .. s-1
   double2* C;                // complex output
   int64_t ldc;
   int Mc, Nc;                // valid complex rows / cols
   const double* row_scale;   // per complex row of op(A)
   const double* col_scale;   // per complex col of op(B)
-  double gscale;             // alpha * 2^-7(d+2)
+  double alpha;
   int accumulate;            // 0: C = result, 1: C += result
   int* err;
 };
+
+// Accumulation groups of one tile: diagonal d, K range [kb0, kb1) of every slice pair (ta, d - ta).
+struct GroupIter {
+  const GemmArgs* g;
+  int d = 0, kb0 = 0;
+  __device__ explicit GroupIter(const GemmArgs* a) : g(a) {}
+  __device__ bool valid() const { return d < g->s; }
+  // (d+1) pairs x chunk bytes x 127^2 must stay below 2^31 in the int32 accumulator
+  __device__ static int chunk(int d) { return max(1, (int)(2147483647.0 / (16129.0 * (d + 1) * BKB))); }
+  __device__ int kb1() const { return min(g->kblocks, kb0 + chunk(d)); }
+  __device__ void next() {
+    kb0 += chunk(d);
+    if (kb0 >= g->kblocks) { kb0 = 0; ++d; }
+  }
+};
+
+__device__ __forceinline__ void tile_coords(const GemmArgs& g, int t, int& mb, int& nb) {
+  if (g.n_fast) { nb = t % g.num_n; mb = t / g.num_n; }
+  else { mb = t % g.num_m; nb = t / g.num_m; }
+}
 
 __global__ void __launch_bounds__(NTHREADS, 1)
     k_gemm_i8(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, const GemmArgs g) {
@@ -152,23 +179,23 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   uint8_t* sA = smem;
   uint8_t* sB = smem + STAGES * A_STAGE;
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + SMEM_TILES);
-  uint64_t* full = bars;                 // [STAGES]
-  uint64_t* empty = bars + STAGES;       // [STAGES]
-  uint64_t* tfull = bars + 2 * STAGES;   // [2]
-  uint64_t* tempty = bars + 2 * STAGES + 2;  // [2]
-  uint64_t* drain = bars + 2 * STAGES + 4;   // MMA drain on the error path
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * STAGES + 5);
+  uint64_t* full = bars;                       // [STAGES]
+  uint64_t* empty = bars + STAGES;             // [STAGES]
+  uint64_t* tfull = bars + 2 * STAGES;         // [NSLOT]
+  uint64_t* tempty = bars + 2 * STAGES + NSLOT;  // [NSLOT]
+  uint64_t* drain = bars + 2 * STAGES + 2 * NSLOT;  // MMA drain on the error path
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * STAGES + 2 * NSLOT + 1);
   volatile int* err = g.err;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
-    for (int s = 0; s < STAGES; ++s) {
-      mbar_init(&full[s], 1);
-      mbar_init(&empty[s], 1);
+    for (int st = 0; st < STAGES; ++st) {
+      mbar_init(&full[st], 1);
+      mbar_init(&empty[st], 1);
     }
-    for (int a = 0; a < 2; ++a) {
+    for (int a = 0; a < NSLOT; ++a) {
       mbar_init(&tfull[a], 1);
-      mbar_init(&tempty[a], 4);  // one arrival per epilogue warp
+      mbar_init(&tempty[a], EPI_WARPS);  // one arrival per epilogue warp
     }
     mbar_init(drain, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -181,31 +208,32 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
-
   const int ntiles = g.num_m * g.num_n;
-  const int npairs = g.diag + 1;
-  const int kspan = g.kb_end - g.kb_begin;
-  const int ksteps = npairs * kspan;
 
   if (warp == 0) {
     if (lane == 0) {
       int stage = 0;
       uint32_t phase = 0;
       bool ok = true;
-      int issued[STAGES];          // parity of the last load issued into each stage (-1: none)
+      int issued[STAGES];  // parity of the last load issued into each stage (-1: none)
       for (int s2 = 0; s2 < STAGES; ++s2) issued[s2] = -1;
       for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-        const int mb = t % g.num_m, nb = t / g.num_m;
-        for (int step = 0; step < ksteps && ok; ++step) {
-          const int ta = step / kspan, kb = g.kb_begin + step % kspan;
-          const int tb = g.diag - ta;
-          ok = mbar_wait(&empty[stage], phase ^ 1, err);
-          if (!ok) break;
-          mbar_expect_tx(&full[stage], A_STAGE + B_STAGE);
-          tma_load_3d(sA + stage * A_STAGE, &mapA, &full[stage], kb * BKB, mb * BM, ta);
-          tma_load_3d(sB + stage * B_STAGE, &mapB, &full[stage], kb * BKB, nb * BN, tb);
-          issued[stage] = (int)phase;
-          if (++stage == STAGES) { stage = 0; phase ^= 1; }
+        int mb, nb;
+        tile_coords(g, t, mb, nb);
+        for (GroupIter gi(&g); gi.valid() && ok; gi.next()) {
+          const int kb1 = gi.kb1();
+          for (int ta = 0; ta <= gi.d && ok; ++ta) {
+            const int tb = gi.d - ta;
+            for (int kb = gi.kb0; kb < kb1; ++kb) {
+              ok = mbar_wait(&empty[stage], phase ^ 1, err);
+              if (!ok) break;
+              mbar_expect_tx(&full[stage], A_STAGE + B_STAGE);
+              tma_load_3d(sA + stage * A_STAGE, &mapA, &full[stage], kb * BKB, mb * BM, ta);
+              tma_load_3d(sB + stage * B_STAGE, &mapB, &full[stage], kb * BKB, nb * BN, tb);
+              issued[stage] = (int)phase;
+              if (++stage == STAGES) { stage = 0; phase ^= 1; }
+            }
+          }
         }
       }
       // every issued copy must land before the CTA may exit (bounded)
@@ -221,29 +249,35 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       const uint32_t idesc = make_idesc();
       int stage = 0;
       uint32_t phase = 0;
-      int lt = 0;
+      int grp = 0;  // accumulation-group counter (selects the TMEM slot)
       bool ok = true;
-      for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++lt) {
-        const int acc = lt & 1;
-        const uint32_t tphase = (lt >> 1) & 1;
-        ok = mbar_wait(&tempty[acc], tphase ^ 1, err);
-        if (!ok) break;
-        tc_fence_after();
-        const uint32_t dtmem = tmem_base + acc * BN;
-        for (int step = 0; step < ksteps; ++step) {
-          ok = mbar_wait(&full[stage], phase, err);
+      for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+        for (GroupIter gi(&g); gi.valid() && ok; gi.next(), ++grp) {
+          const int acc = grp % NSLOT;
+          ok = mbar_wait(&tempty[acc], ((grp / NSLOT) & 1) ^ 1, err);
           if (!ok) break;
           tc_fence_after();
-          const uint32_t a0 = smem_u32(sA + stage * A_STAGE), b0 = smem_u32(sB + stage * B_STAGE);
+          const uint32_t dtmem = tmem_base + acc * BN;
+          const int kb1 = gi.kb1();
+          bool first = true;
+          for (int ta = 0; ta <= gi.d && ok; ++ta) {
+            for (int kb = gi.kb0; kb < kb1; ++kb) {
+              ok = mbar_wait(&full[stage], phase, err);
+              if (!ok) break;
+              tc_fence_after();
+              const uint32_t a0 = smem_u32(sA + stage * A_STAGE), b0 = smem_u32(sB + stage * B_STAGE);
 #pragma unroll
-          for (int kk = 0; kk < BKB / 32; ++kk) {
-            umma_i8(dtmem, make_desc(a0 + kk * 32), make_desc(b0 + kk * 32), idesc, (step > 0 || kk > 0) ? 1u : 0u);
+              for (int kk = 0; kk < BKB / 32; ++kk) {
+                umma_i8(dtmem, make_desc(a0 + kk * 32), make_desc(b0 + kk * 32), idesc, first ? 0u : 1u);
+                first = false;
+              }
+              umma_commit(&empty[stage]);  // frees the smem stage when these MMAs retire
+              if (++stage == STAGES) { stage = 0; phase ^= 1; }
+            }
           }
-          umma_commit(&empty[stage]);  // frees the smem stage when these MMAs retire
-          if (++stage == STAGES) { stage = 0; phase ^= 1; }
+          if (!ok) break;
+          umma_commit(&tfull[acc]);
         }
-        if (!ok) break;
-        umma_commit(&tfull[acc]);
       }
       // all MMAs issued by this thread retire before TMEM is released (bounded)
       umma_commit(drain);
@@ -252,42 +286,56 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       }
     }
   } else {
-    // epilogue warps 2..5: TMEM lane quarter = warp % 4
+    // epilogue warps 2..9: TMEM lane quarter q = warp % 4, column half h
+    constexpr int HC = BN / 2;  // columns per epilogue thread
     const int q = warp & 3;
+    const int h = (warp - 2) / 4;
     const int row = q * 32 + lane;  // tile row == TMEM lane
-    int lt = 0;
-    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++lt) {
-      const int acc = lt & 1;
-      const uint32_t tphase = (lt >> 1) & 1;
-      if (!mbar_wait(&tfull[acc], tphase, err)) break;
-      tc_fence_after();
-      const int mb = t % g.num_m, nb = t / g.num_m;
-      const int rr = mb * BM + row;           // real row of At
-      const int ci = rr >> 1, part = rr & 1;  // complex row, re/im
-      const bool rvalid = ci < g.Mc;
-      const double rs = rvalid ? g.row_scale[ci] * g.gscale : 0.0;
-      double* Cd = reinterpret_cast<double*>(g.C);
-      for (int cc = 0; cc < BN / 32; ++cc) {
-        int32_t r[32];
-        tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + acc * BN + cc * 32, r);
-        if (rvalid) {
+    double* Cd = reinterpret_cast<double*>(g.C);
+    int grp = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+      int mb, nb;
+      tile_coords(g, t, mb, nb);
+      // FP64 partial sums of this thread's row over all slice diagonals of the tile
+      double part[HC];
 #pragma unroll
-          for (int j = 0; j < 32; ++j) {
-            const int cj = nb * BN + cc * 32 + j;
-            if (cj < g.Nc) {
-              double v = (double)r[j] * rs * g.col_scale[cj];
-              double* p = Cd + 2 * ((int64_t)ci + g.ldc * cj) + part;
-              *p = g.accumulate ? (*p + v) : v;
-            }
+      for (int j = 0; j < HC; ++j) part[j] = 0.0;
+      bool ok = true;
+      for (GroupIter gi(&g); gi.valid(); gi.next(), ++grp) {
+        const int acc = grp % NSLOT;
+        if (!mbar_wait(&tfull[acc], (grp / NSLOT) & 1, err)) { ok = false; break; }
+        tc_fence_after();
+        const double w = ldexp(1.0, -7 * (gi.d + 2));
+#pragma unroll
+        for (int cc = 0; cc < HC / 32; ++cc) {
+          int32_t r[32];
+          tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + acc * BN + h * HC + cc * 32, r);
+#pragma unroll
+          for (int j = 0; j < 32; ++j) part[cc * 32 + j] = fma((double)r[j], w, part[cc * 32 + j]);
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&tempty[acc]);
+      }
+      if (!ok) break;
+      const int rr = mb * BM + row;           // real row of At
+      const int ci = rr >> 1, part_im = rr & 1;  // complex row, re/im
+      if (ci < g.Mc) {
+        const double rs = g.row_scale[ci] * g.alpha;
+#pragma unroll
+        for (int j = 0; j < HC; ++j) {
+          const int cj = nb * BN + h * HC + j;
+          if (cj < g.Nc) {
+            const double v = part[j] * rs * __ldg(&g.col_scale[cj]);
+            double* p = Cd + 2 * ((int64_t)ci + g.ldc * cj) + part_im;
+            *p = g.accumulate ? (*p + v) : v;
           }
         }
       }
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&tempty[acc]);
     }
   }
-  // drain: make sure every MMA of this CTA retired before releasing TMEM
+  // TMEM is released only after every MMA of this CTA retired (epilogue saw all
+  // groups, or the MMA thread drained on the error path)
   __syncthreads();
   if (warp == 1) {
     tc_fence_after();
@@ -556,7 +604,7 @@ void split_operand_b(Context* ctx, SplitOperand& S, Op op, int K, int N, const d
 void split_gemm(Context* ctx, const SplitOperand& A, const SplitOperand& B, int s, double alpha, bool accumulate,
                 dcplx* C, int64_t ldc) {
   IMPS_REQUIRE(A.K == B.K && A.Kp == B.Kp, IMPS_DIM_MISMATCH, "split_gemm: inner dimensions differ");
-  IMPS_REQUIRE(s <= A.s && s <= B.s, IMPS_INVALID_ARG, "split_gemm: more slices requested than stored");
+  IMPS_REQUIRE(s >= 1 && s <= A.s && s <= B.s && s <= 8, IMPS_INVALID_ARG, "split_gemm: bad slice count");
   static bool attr = false;
   if (!attr) {
     IMPS_CUDA(cudaFuncSetAttribute(k_gemm_i8, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
@@ -569,35 +617,28 @@ void split_gemm(Context* ctx, const SplitOperand& A, const SplitOperand& B, int 
   GemmArgs g;
   g.num_m = (int)(A.Rp / BM);
   g.num_n = (int)(B.Rp / BN);
+  // stream the larger operand once: consecutive CTAs share its tile and walk the other
+  g.n_fast = (A.Rp * A.s >= B.Rp * B.s) ? 1 : 0;
   g.kblocks = (int)(A.Kp / BKB);
+  g.s = s;
   g.C = C;
   g.ldc = ldc;
   g.Mc = A.rows;
   g.Nc = B.rows;
   g.row_scale = A.scale.d();
   g.col_scale = B.scale.d();
+  g.alpha = alpha;
+  g.accumulate = accumulate ? 1 : 0;
   g.err = static_cast<int*>(errb.ptr);
-  // K chunk bound: (d+1) * chunk_bytes * 127^2 < 2^31  ->  per diagonal
   const int ntiles = g.num_m * g.num_n;
   const int grid = std::max(1, std::min(ntiles, ctx->num_sms));
-  bool first = true;
-  for (int d = 0; d < s; ++d) {
-    const int64_t max_k_bytes = (int64_t)(2147483647.0 / (16129.0 * (d + 1)));
-    const int kbchunk = (int)std::max<int64_t>(1, max_k_bytes / BKB);
-    for (int kb0 = 0; kb0 < g.kblocks; kb0 += kbchunk) {
-      g.diag = d;
-      g.kb_begin = kb0;
-      g.kb_end = std::min(g.kblocks, kb0 + kbchunk);
-      g.gscale = alpha * std::ldexp(1.0, -7 * (d + 2));
-      g.accumulate = (first && !accumulate) ? 0 : 1;
-      first = false;
-      ScopedTimer tm(ctx, "gemm_split",
-                     2.0 * (double)A.Rp * (double)B.Rp * (double)(g.kb_end - g.kb_begin) * BKB * (d + 1));
-      k_gemm_i8<<<grid, NTHREADS, SMEM_BYTES, ctx->stream>>>(mapA, mapB, g);
-      ctx->n_kernels++;
-      ctx->n_gemm++;
-      IMPS_CUDA(cudaPeekAtLastError());
-    }
+  {
+    ScopedTimer tm(ctx, "gemm_split",
+                   2.0 * (double)A.Rp * (double)B.Rp * (double)A.Kp * (double)(s * (s + 1) / 2));
+    k_gemm_i8<<<grid, NTHREADS, SMEM_BYTES, ctx->stream>>>(mapA, mapB, g);
+    ctx->n_kernels++;
+    ctx->n_gemm++;
+    IMPS_CUDA(cudaPeekAtLastError());
   }
   int herr = 0;
   IMPS_CUDA(cudaMemcpyAsync(&herr, errb.ptr, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
