@@ -113,6 +113,10 @@ int imps_ctx_profile(imps_ctx* ctx, int enable);
 int imps_ctx_profile_get(imps_ctx* ctx, const char* kernel_class, int64_t* launches, double* total_ms,
                          double* work);
 int imps_ctx_profile_reset(imps_ctx* ctx);
+/* Restrict timing to a comma-separated list of kernel classes (NULL or "" = all). */
+int imps_ctx_profile_classes(imps_ctx* ctx, const char* csv);
+/* Every kernel class seen so far as text lines "class[@call-site] launches total_ms work". */
+int imps_ctx_profile_dump(imps_ctx* ctx, char* buf, int64_t len);
 /* counters[0..4] = AC applies, C applies, pushes, GEMM launches, all kernel launches */
 int imps_ctx_counters(imps_ctx* ctx, int64_t* counters);
 

@@ -83,6 +83,8 @@ _SIGS = {
     "imps_ctx_profile": (I32, [P, I32]),
     "imps_ctx_profile_get": (I32, [P, C.c_char_p, C.POINTER(I64), DP, DP]),
     "imps_ctx_profile_reset": (I32, [P]),
+    "imps_ctx_profile_dump": (I32, [P, C.c_char_p, I64]),
+    "imps_ctx_profile_classes": (I32, [P, C.c_char_p]),
     "imps_ctx_counters": (I32, [P, C.POINTER(I64)]),
     "imps_mpo_create": (I32, [P, I32, C.POINTER(I32), C.POINTER(I32), C.POINTER(I32), C.POINTER(DP), PP]),
     "imps_mpo_destroy": (I32, [P]),

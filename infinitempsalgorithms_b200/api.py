@@ -130,6 +130,11 @@ class Context:
     def profile(self, enable: bool = True):
         check(self.lib.imps_ctx_profile(self.h, int(enable)), self.h)
 
+    def profile_classes(self, classes=None):
+        """Time only these kernel classes (None: all)."""
+        csv = ",".join(classes) if classes else None
+        check(self.lib.imps_ctx_profile_classes(self.h, csv.encode() if csv else None), self.h)
+
     def profile_reset(self):
         check(self.lib.imps_ctx_profile_reset(self.h), self.h)
 
@@ -139,6 +144,16 @@ class Context:
         work = C.c_double()
         check(self.lib.imps_ctx_profile_get(self.h, cls.encode(), C.byref(n), C.byref(ms), C.byref(work)), self.h)
         return n.value, ms.value, work.value
+
+    def profile_dump(self):
+        """{class@site: (launches, total_ms, work)} for every kernel class timed so far."""
+        buf = C.create_string_buffer(1 << 16)
+        check(self.lib.imps_ctx_profile_dump(self.h, buf, len(buf)), self.h)
+        out = {}
+        for line in buf.value.decode().splitlines():
+            name, n, ms, work = line.split()
+            out[name] = (int(n), float(ms), float(work))
+        return out
 
     def counters(self):
         arr = (C.c_int64 * 5)()

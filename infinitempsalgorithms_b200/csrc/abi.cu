@@ -137,6 +137,7 @@ int imps_ctx_destroy(imps_ctx* h) {
     cudaEventDestroy(p.second.first);
     cudaEventDestroy(p.second.second);
   }
+  for (auto e : c.event_pool) cudaEventDestroy(e);
   c.scratch.clear();
   c.red.release();
   if (c.host_pinned) cudaFreeHost(c.host_pinned);
@@ -200,8 +201,8 @@ static void flush_profile(imps::Context& c) {
     s.launches++;
     s.ms += ms;
     s.flops += c.pending_flops[i];
-    cudaEventDestroy(c.pending[i].second.first);
-    cudaEventDestroy(c.pending[i].second.second);
+    c.event_pool.push_back(c.pending[i].second.first);
+    c.event_pool.push_back(c.pending[i].second.second);
   }
   c.pending.clear();
   c.pending_flops.clear();
@@ -215,6 +216,37 @@ int imps_ctx_profile_get(imps_ctx* h, const char* cls, int64_t* launches, double
     if (launches) *launches = it == h->c.stats.end() ? 0 : it->second.launches;
     if (total_ms) *total_ms = it == h->c.stats.end() ? 0.0 : it->second.ms;
     if (work) *work = it == h->c.stats.end() ? 0.0 : it->second.flops;
+    return IMPS_OK;
+  });
+}
+
+int imps_ctx_profile_classes(imps_ctx* h, const char* csv) {
+  if (!h) return IMPS_INVALID_ARG;
+  h->c.profile_only.clear();
+  if (csv) {
+    std::string s(csv), cur;
+    for (char ch : s) {
+      if (ch == ',') { if (!cur.empty()) h->c.profile_only.insert(cur); cur.clear(); }
+      else cur += ch;
+    }
+    if (!cur.empty()) h->c.profile_only.insert(cur);
+  }
+  return IMPS_OK;
+}
+
+int imps_ctx_profile_dump(imps_ctx* h, char* buf, int64_t len) {
+  if (!h || !buf || len <= 0) return IMPS_INVALID_ARG;
+  return guard(&h->c, [&] {
+    flush_profile(h->c);
+    std::string out;
+    for (auto& kv : h->c.stats) {
+      char line[256];
+      snprintf(line, sizeof(line), "%s %lld %.6f %.6e\n", kv.first.c_str(), (long long)kv.second.launches,
+               kv.second.ms, kv.second.flops);
+      out += line;
+    }
+    IMPS_REQUIRE((int64_t)out.size() < len, IMPS_INVALID_ARG, "profile dump buffer too small");
+    std::memcpy(buf, out.c_str(), out.size() + 1);
     return IMPS_OK;
   });
 }

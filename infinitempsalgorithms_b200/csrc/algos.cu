@@ -27,6 +27,7 @@ double dyn_tol(double eps, double factor, int iter) {
 
 double galerkin(Context* ctx, imps_envs* E, const imps_mpo* H, const imps_state* st) {
   Fp64Scope fp64(ctx);  // the Galerkin residual is always FP64
+  ProfTag tag(ctx, "galerkin");
   double eps = 0.0;
   for (int site = 0; site < st->N; ++site) {
     const int Dl = st->Dl(site), d = st->d[site], Dr = st->Dr(site);
@@ -47,6 +48,7 @@ double galerkin(Context* ctx, imps_envs* E, const imps_mpo* H, const imps_state*
 
 cplx energy(Context* ctx, imps_envs* E, const imps_mpo* H, imps_state* st) {
   Fp64Scope fp64(ctx);
+  ProfTag tag(ctx, "energy");
   cplx e = 0.0;
   for (int site = 0; site < st->N; ++site) {
     const MpoSite& col = H->closing[site % H->N];
@@ -113,6 +115,7 @@ KrylovResult eigsolve_ac(Context* ctx, imps_envs* E, const imps_mpo* H, int site
                          double tol, int kdim, int maxiter, bool eager) {
   const int64_t n = (int64_t)E->Dl[site] * H->sites[site % H->N].d * E->Dr[site];
   ConstScope cs(ctx, {E->lefts[site].ptr, E->rights[site].ptr});
+  ProfTag tag(ctx, "eig_ac");
   LinOp op = [&](const dcplx* v, dcplx* out) { ac_apply(ctx, E, H, site, v, out); };
   return mixed_eigsolve(ctx, n, op, x0, x, tol, kdim, maxiter, eager, E->hest_ac[site]);
 }
@@ -123,6 +126,7 @@ KrylovResult eigsolve_c(Context* ctx, imps_envs* E, int site, const dcplx* x0, d
   const int l1 = (site + 1) % E->N;
   ensure_GLp(ctx, E, l1);
   ConstScope cs(ctx, {E->GLp[l1].ptr, E->rights[site].ptr});
+  ProfTag tag(ctx, "eig_c");
   LinOp op = [&](const dcplx* v, dcplx* out) { c_apply(ctx, E, site, v, out); };
   return mixed_eigsolve(ctx, n, op, x0, x, tol, kdim, maxiter, eager, E->hest_c[site]);
 }
@@ -160,6 +164,7 @@ void vumps_localupdate(Context* ctx, imps_envs* E, const imps_mpo* H, imps_state
     KrylovResult r2 = eigsolve_c(ctx, E, site, st->C[site].z(), c.z(), tol, kdim, maxiter, eager);
     ac_ops += r1.numops;
     c_ops += r2.numops;
+    ProfTag tag(ctx, "regauge");
     regauge(ctx, Dl, d, Dr, ac.z(), c.z(), st->AL[site].z());
   }
   if (nac) *nac = ac_ops;
@@ -174,8 +179,16 @@ imps_vumps_info vumps_iter(Context* ctx, imps_envs* E, const imps_mpo* H, imps_s
   const int N = st->N, DN = st->Dr(N - 1);
   DevBuf& c0 = ctx->buf("vumps_c0", (size_t)DN * DN * sizeof(dcplx));
   zcopy(ctx, (int64_t)DN * DN, st->C[N - 1].z(), c0.z());
-  GaugeResult g = from_al(ctx, st, c0.z(), dyn_tol(eps, 1e-6, siter), 300);
-  imps_env_info ei = envs_build(ctx, E, st, H, dyn_tol(eps, 1e-4, siter), 300, 30, true);
+  GaugeResult g;
+  {
+    ProfTag tag(ctx, "gauge");
+    g = from_al(ctx, st, c0.z(), dyn_tol(eps, 1e-6, siter), 300);
+  }
+  imps_env_info ei;
+  {
+    ProfTag tag(ctx, "envs");
+    ei = envs_build(ctx, E, st, H, dyn_tol(eps, 1e-4, siter), 300, 30, true);
+  }
   info.galerkin = galerkin(ctx, E, H, st);
   cplx e = energy(ctx, E, H, st);
   info.energy_re = e.real();

@@ -416,87 +416,108 @@ __device__ __forceinline__ void slice_value(double x, int s, int8_t* out) {
   }
 }
 
-// Split op(A) into expanded K-major planes.  Element (i, k) of op(A); each thread
-// produces 2 real rows x 2 real cols (4 bytes in 2 rows) per plane.
-// opA == 0: A[i + lda k] (tile-transposed through shared memory), opA == 2: conj(A[k + lda i]).
+// Split op(A) into expanded K-major planes.  A block covers 32 complex rows x 64
+// complex k of the *padded* extent (so no separate zero fill is needed); each
+// thread slices 4 consecutive complex k and stores 8 bytes into each of the two
+// expanded rows per plane.
+// opA == 0: A[i + lda k] (transposed through shared memory), opA == 2: conj(A[k + lda i]).
 template <int OPA>
-__global__ void k_split_a(int M, int K, const double2* __restrict__ A, int64_t lda, const double* __restrict__ inv,
-                          int s, int8_t* __restrict__ out, int64_t Kp, int64_t plane) {
-  __shared__ double2 tile[32][33];
-  const int i0 = blockIdx.y * 32, k0 = blockIdx.x * 32;
-  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
-  for (int r = ty; r < 32; r += 8) {
-    int i, k;
-    double2 v = make_double2(0.0, 0.0);
-    if (OPA == 0) {
-      i = i0 + tx; k = k0 + r;
-      if (i < M && k < K) v = A[i + lda * k];
-      tile[tx][r] = v;   // tile[i_local][k_local]
-    } else {
-      k = k0 + tx; i = i0 + r;
-      if (i < M && k < K) { v = A[k + lda * i]; v.y = -v.y; }
-      tile[r][tx] = v;
+__global__ void __launch_bounds__(256) k_split_a(int M, int K, const double2* __restrict__ A, int64_t lda,
+                                                 const double* __restrict__ inv, int s, int8_t* __restrict__ out,
+                                                 int64_t Kp, int64_t plane) {
+  __shared__ double2 tile[32][65];
+  const int i0 = blockIdx.y * 32, k0 = blockIdx.x * 64;
+  const int tid = threadIdx.x;
+  if (OPA == 0) {
+    const int tx = tid & 31, ty = tid >> 5;
+    for (int r = ty; r < 64; r += 8) {
+      const int i = i0 + tx, k = k0 + r;
+      tile[tx][r] = (i < M && k < K) ? A[i + lda * k] : make_double2(0.0, 0.0);
+    }
+  } else {
+    const int kx = tid & 63, iy = tid >> 6;
+    for (int r = iy; r < 32; r += 4) {
+      const int i = i0 + r, k = k0 + kx;
+      double2 v = (i < M && k < K) ? A[k + lda * i] : make_double2(0.0, 0.0);
+      v.y = -v.y;
+      tile[r][kx] = v;
     }
   }
   __syncthreads();
-  // write: real rows 2i, 2i+1; real cols 2k, 2k+1.  Thread (tx = k_local, ty) handles rows i_local = ty + 8j
-  for (int il = ty; il < 32; il += 8) {
-    const int i = i0 + il, k = k0 + tx;
-    if (i >= M) continue;
-    const double2 v = tile[il][tx];
-    const double sc = inv[i];
-    int8_t re[8], im[8];
-    slice_value(v.x * sc, s, re);
-    slice_value(v.y * sc, s, im);
+  for (int item = tid; item < 32 * 16; item += 256) {
+    const int il = item >> 4, kq = item & 15;
+    const int i = i0 + il;
+    const double sc = (i < M) ? inv[i] : 0.0;
+    int8_t re[4][8], im[4][8];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const double2 v = tile[il][4 * kq + c];
+      slice_value(v.x * sc, s, re[c]);
+      slice_value(v.y * sc, s, im[c]);
+    }
+    int8_t* p0 = out + (int64_t)(2 * i) * Kp + 2 * (k0 + 4 * kq);
     for (int t = 0; t < s; ++t) {
-      // row 2i: (Re, -Im); row 2i+1: (Im, Re)
-      int8_t* p0 = out + plane * t + (int64_t)(2 * i) * Kp + 2 * k;
-      int8_t* p1 = p0 + Kp;
-      char2 w0, w1;
-      w0.x = (k < K) ? re[t] : 0;
-      w0.y = (k < K) ? (int8_t)(-im[t]) : 0;
-      w1.x = (k < K) ? im[t] : 0;
-      w1.y = (k < K) ? re[t] : 0;
-      *reinterpret_cast<char2*>(p0) = w0;
-      *reinterpret_cast<char2*>(p1) = w1;
+      // row 2i: (Re, -Im) pairs; row 2i+1: (Im, Re) pairs
+      uint32_t lo0 = 0, hi0 = 0, lo1 = 0, hi1 = 0;
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        lo0 |= ((uint32_t)(uint8_t)re[c][t] | ((uint32_t)(uint8_t)(int8_t)(-im[c][t]) << 8)) << (16 * c);
+        hi0 |= ((uint32_t)(uint8_t)re[c + 2][t] | ((uint32_t)(uint8_t)(int8_t)(-im[c + 2][t]) << 8)) << (16 * c);
+        lo1 |= ((uint32_t)(uint8_t)im[c][t] | ((uint32_t)(uint8_t)re[c][t] << 8)) << (16 * c);
+        hi1 |= ((uint32_t)(uint8_t)im[c + 2][t] | ((uint32_t)(uint8_t)re[c + 2][t] << 8)) << (16 * c);
+      }
+      *reinterpret_cast<uint2*>(p0 + plane * t) = make_uint2(lo0, hi0);
+      *reinterpret_cast<uint2*>(p0 + plane * t + Kp) = make_uint2(lo1, hi1);
     }
   }
 }
 
-// Split op(B) (K x N complex) into K-major planes Bt[j][2k + p].
+// Split op(B) (K x N complex) into K-major planes Bt[j][2k + p], same tiling over
+// the padded extent; 8-byte stores of 4 consecutive complex k.
 // opB == 0: B[k + ldb j] (contiguous in k); opB == 2: conj(B[j + ldb k]) (tile transpose).
 template <int OPB>
-__global__ void k_split_b(int K, int N, const double2* __restrict__ B, int64_t ldb, const double* __restrict__ inv,
-                          int s, int8_t* __restrict__ out, int64_t Kp, int64_t plane) {
-  __shared__ double2 tile[32][33];
-  const int j0 = blockIdx.y * 32, k0 = blockIdx.x * 32;
-  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-  for (int r = ty; r < 32; r += 8) {
-    double2 v = make_double2(0.0, 0.0);
-    if (OPB == 0) {
-      int k = k0 + tx, j = j0 + r;
-      if (k < K && j < N) v = B[k + ldb * j];
-      tile[r][tx] = v;  // tile[j_local][k_local]
-    } else {
-      int j = j0 + tx, k = k0 + r;
-      if (k < K && j < N) { v = B[j + ldb * k]; v.y = -v.y; }
+__global__ void __launch_bounds__(256) k_split_b(int K, int N, const double2* __restrict__ B, int64_t ldb,
+                                                 const double* __restrict__ inv, int s, int8_t* __restrict__ out,
+                                                 int64_t Kp, int64_t plane) {
+  __shared__ double2 tile[32][65];
+  const int j0 = blockIdx.y * 32, k0 = blockIdx.x * 64;
+  const int tid = threadIdx.x;
+  if (OPB == 0) {
+    const int kx = tid & 63, jy = tid >> 6;
+    for (int r = jy; r < 32; r += 4) {
+      const int j = j0 + r, k = k0 + kx;
+      tile[r][kx] = (k < K && j < N) ? B[k + ldb * j] : make_double2(0.0, 0.0);
+    }
+  } else {
+    const int tx = tid & 31, ty = tid >> 5;
+    for (int r = ty; r < 64; r += 8) {
+      const int j = j0 + tx, k = k0 + r;
+      double2 v = (k < K && j < N) ? B[j + ldb * k] : make_double2(0.0, 0.0);
+      v.y = -v.y;
       tile[tx][r] = v;
     }
   }
   __syncthreads();
-  for (int jl = ty; jl < 32; jl += 8) {
-    const int j = j0 + jl, k = k0 + tx;
-    if (j >= N) continue;
-    const double2 v = tile[jl][tx];
-    const double sc = inv[j];
-    int8_t re[8], im[8];
-    slice_value(v.x * sc, s, re);
-    slice_value(v.y * sc, s, im);
+  for (int item = tid; item < 32 * 16; item += 256) {
+    const int jl = item >> 4, kq = item & 15;
+    const int j = j0 + jl;
+    const double sc = (j < N) ? inv[j] : 0.0;
+    int8_t re[4][8], im[4][8];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const double2 v = tile[jl][4 * kq + c];
+      slice_value(v.x * sc, s, re[c]);
+      slice_value(v.y * sc, s, im[c]);
+    }
+    int8_t* p0 = out + (int64_t)j * Kp + 2 * (k0 + 4 * kq);
     for (int t = 0; t < s; ++t) {
-      char2 w;
-      w.x = (k < K) ? re[t] : 0;
-      w.y = (k < K) ? im[t] : 0;
-      *reinterpret_cast<char2*>(out + plane * t + (int64_t)j * Kp + 2 * k) = w;
+      uint32_t lo = 0, hi = 0;
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        lo |= ((uint32_t)(uint8_t)re[c][t] | ((uint32_t)(uint8_t)im[c][t] << 8)) << (16 * c);
+        hi |= ((uint32_t)(uint8_t)re[c + 2][t] | ((uint32_t)(uint8_t)im[c + 2][t] << 8)) << (16 * c);
+      }
+      *reinterpret_cast<uint2*>(p0 + plane * t) = make_uint2(lo, hi);
     }
   }
 }
@@ -547,7 +568,6 @@ void split_operand_a(Context* ctx, SplitOperand& S, Op op, int M, int K, const d
   S.inv.ensure((size_t)M * sizeof(double));
   S.mx.ensure((size_t)M * sizeof(unsigned long long));
   ScopedTimer tm(ctx, "split_slice", 16.0 * M * K + (double)plane * s);
-  IMPS_CUDA(cudaMemsetAsync(S.data.ptr, 0, plane * s, ctx->stream));
   IMPS_CUDA(cudaMemsetAsync(S.mx.ptr, 0, (size_t)M * 8, ctx->stream));
   auto* mx = static_cast<unsigned long long*>(S.mx.ptr);
   if (op == OP_N) {
@@ -558,7 +578,8 @@ void split_operand_a(Context* ctx, SplitOperand& S, Op op, int M, int K, const d
     k_linemax_contig<<<(M + 7) / 8, 256, 0, ctx->stream>>>(M, K, A, lda, mx);
   }
   k_scales<<<(M + 255) / 256, 256, 0, ctx->stream>>>(M, mx, S.scale.d(), S.inv.d());
-  dim3 g2((K + 31) / 32, (M + 31) / 32);
+  // grid over the padded extent: Kp / 2 complex columns, Rp / 2 complex rows
+  dim3 g2((unsigned)(S.Kp / 2 / 64), (unsigned)(S.Rp / 2 / 32));
   if (op == OP_N)
     k_split_a<0><<<g2, 256, 0, ctx->stream>>>(M, K, A, lda, S.inv.d(), s, static_cast<int8_t*>(S.data.ptr), S.Kp, plane);
   else
@@ -581,7 +602,6 @@ void split_operand_b(Context* ctx, SplitOperand& S, Op op, int K, int N, const d
   S.inv.ensure((size_t)N * sizeof(double));
   S.mx.ensure((size_t)N * sizeof(unsigned long long));
   ScopedTimer tm(ctx, "split_slice", 16.0 * K * N + (double)plane * s);
-  IMPS_CUDA(cudaMemsetAsync(S.data.ptr, 0, plane * s, ctx->stream));
   IMPS_CUDA(cudaMemsetAsync(S.mx.ptr, 0, (size_t)N * 8, ctx->stream));
   auto* mx = static_cast<unsigned long long*>(S.mx.ptr);
   if (op == OP_N) {
@@ -592,7 +612,7 @@ void split_operand_b(Context* ctx, SplitOperand& S, Op op, int K, int N, const d
     k_colmax_strided<<<g, 128, 0, ctx->stream>>>(N, K, B, ldb, kchunk, mx);
   }
   k_scales<<<(N + 255) / 256, 256, 0, ctx->stream>>>(N, mx, S.scale.d(), S.inv.d());
-  dim3 g2((K + 31) / 32, (N + 31) / 32);
+  dim3 g2((unsigned)(S.Kp / 2 / 64), (unsigned)(S.Rp / 32));
   if (op == OP_N)
     k_split_b<0><<<g2, 256, 0, ctx->stream>>>(K, N, B, ldb, S.inv.d(), s, static_cast<int8_t*>(S.data.ptr), S.Kp, plane);
   else

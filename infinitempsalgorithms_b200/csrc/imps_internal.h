@@ -119,6 +119,9 @@ struct Context {
   int* dev_info = nullptr;
   // profiling
   bool profile = false;
+  const char* prof_tag = "";           // call-site tag appended to kernel classes when profiling
+  std::set<std::string> profile_only;  // when non-empty, only these kernel classes are timed
+  std::vector<cudaEvent_t> event_pool; // reusable timing events
   std::map<std::string, KernelStat> stats;
   std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
   double pending_flops_dummy = 0;
@@ -161,6 +164,13 @@ struct ConstScope {
       }
     }
   }
+};
+// Tags the kernels launched while alive with a call site (profiling attribution).
+struct ProfTag {
+  Context* ctx;
+  const char* old;
+  ProfTag(Context* c, const char* tag) : ctx(c), old(c->prof_tag) { ctx->prof_tag = tag; }
+  ~ProfTag() { ctx->prof_tag = old; }
 };
 // Forces FP64 for every GEMM while alive.
 struct Fp64Scope {
@@ -292,6 +302,8 @@ double dznrm2(Context* ctx, int64_t n, const dcplx* x);
 cplx zdotc(Context* ctx, int64_t n, const dcplx* x, const dcplx* y);  // sum conj(x) y
 // h[j] = sum_k conj(V[k + ldv j]) w[k], j < nv  (one fused pass over V)
 void zdotc_multi(Context* ctx, int64_t n, int nv, const dcplx* V, int64_t ldv, const dcplx* w, cplx* h_host);
+// same, and returns ||w|| from the same pass over w
+double zdotc_multi_norm(Context* ctx, int64_t n, int nv, const dcplx* V, int64_t ldv, const dcplx* w, cplx* h_host);
 // w += sum_j coef[j] V[:, j]
 void zgemv_acc(Context* ctx, int64_t n, int nv, const dcplx* V, int64_t ldv, const cplx* coef, dcplx* w);
 // y = sum_j coef[j] V[:, j]

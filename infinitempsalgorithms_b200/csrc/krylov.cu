@@ -18,19 +18,28 @@
 namespace imps {
 namespace {
 
-// w <- w - V h, twice; returns h1 + h2 (host) for the nv basis vectors.
-void cgs2(Context* ctx, int64_t n, int nv, const dcplx* V, dcplx* w, std::vector<cplx>& h) {
+// Classical Gram-Schmidt with the DGKS criterion: w <- w - V h; a second pass runs
+// only if the first one removed more than 1 - 1/sqrt(2) of the norm of w.  Returns
+// the coefficients (host) and ||w|| after orthogonalisation.
+double cgs2(Context* ctx, int64_t n, int nv, const dcplx* V, dcplx* w, std::vector<cplx>& h) {
   h.assign(nv, cplx(0.0, 0.0));
-  if (nv == 0) return;
+  if (nv == 0) return dznrm2(ctx, n, w);
   std::vector<cplx> h1(nv), neg(nv);
+  double nw = zdotc_multi_norm(ctx, n, nv, V, n, w, h1.data());
   for (int pass = 0; pass < 2; ++pass) {
-    zdotc_multi(ctx, n, nv, V, n, w, h1.data());
     for (int j = 0; j < nv; ++j) {
       neg[j] = -h1[j];
       h[j] += h1[j];
     }
     zgemv_acc(ctx, n, nv, V, n, neg.data(), w);
+    if (pass == 1) break;
+    double nproj = 0.0;
+    for (int j = 0; j < nv; ++j) nproj += std::norm(h1[j]);
+    const double nrest2 = nw * nw - nproj;  // ||w - V h||^2 in exact arithmetic
+    if (nrest2 > 0.5 * nw * nw) return dznrm2(ctx, n, w);
+    nw = zdotc_multi_norm(ctx, n, nv, V, n, w, h1.data());
   }
+  return dznrm2(ctx, n, w);
 }
 
 std::vector<cplx> herm_part(const std::vector<cplx>& H, int ldh, int m) {
@@ -72,8 +81,7 @@ KrylovResult lanczos_eigsolve(Context* ctx, int64_t n, const LinOp& A, const dcp
     dcplx* w = V + n * (int64_t)nvec;
     A(V + n * (int64_t)k, w);
     res.numops++;
-    cgs2(ctx, n, nvec, V, w, h);
-    double beta = dznrm2(ctx, n, w);
+    double beta = cgs2(ctx, n, nvec, V, w, h);
     for (int i = 0; i <= k; ++i) H[i + (size_t)ldh * k] = h[i];
     H[k + 1 + (size_t)ldh * k] = beta;
     const int m = k + 1;
@@ -168,8 +176,7 @@ KrylovResult gmres(Context* ctx, int64_t n, const LinOp& A, const dcplx* b, dcpl
     for (int k = 0; k < kdim; ++k) {
       dcplx* w = V + n * (int64_t)(k + 1);
       op(V + n * (int64_t)k, w);
-      cgs2(ctx, n, k + 1, V, w, h);
-      double hn = dznrm2(ctx, n, w);
+      double hn = cgs2(ctx, n, k + 1, V, w, h);
       std::vector<cplx> col(k + 2, 0.0);
       for (int i = 0; i <= k; ++i) col[i] = h[i];
       col[k + 1] = hn;
@@ -243,8 +250,7 @@ KrylovResult exponentiate(Context* ctx, int64_t n, const LinOp& A, cplx t, const
       dcplx* w = V + n * (int64_t)(k + 1);
       A(V + n * (int64_t)k, w);
       res.numops++;
-      cgs2(ctx, n, k + 1, V, w, h);
-      double hn = dznrm2(ctx, n, w);
+      double hn = cgs2(ctx, n, k + 1, V, w, h);
       for (int i = 0; i <= k; ++i) H[i + (size_t)ldh * k] = h[i];
       H[k + 1 + (size_t)ldh * k] = hn;
       m = k + 1;
@@ -298,8 +304,7 @@ KrylovResult arnoldi_dominant(Context* ctx, int64_t n, const LinOp& A, const dcp
     dcplx* w = V + n * (int64_t)nvec;
     A(V + n * (int64_t)k, w);
     res.numops++;
-    cgs2(ctx, n, nvec, V, w, h);
-    double hn = dznrm2(ctx, n, w);
+    double hn = cgs2(ctx, n, nvec, V, w, h);
     for (int i = 0; i <= k; ++i) H[i + (size_t)ldh * k] = h[i];
     H[k + 1 + (size_t)ldh * k] = hn;
     const int m = k + 1;

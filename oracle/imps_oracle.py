@@ -344,12 +344,16 @@ class KrylovInfo:
 
 
 def _cgs2(V: List[np.ndarray], w: np.ndarray):
-    """Classical Gram-Schmidt with one re-orthogonalisation pass (CGS2)."""
+    """Classical Gram-Schmidt with the DGKS criterion: a second pass only when the
+    first one removed more than 1 - 1/sqrt(2) of ||w|| (||w - V h||^2 <= ||w||^2 / 2)."""
     if not V:
         return w, np.zeros(0, dtype=C128)
     B = np.stack(V, axis=1)
+    nw2 = np.vdot(w, w).real
     h = B.conj().T @ w
     w = w - B @ h
+    if nw2 - np.vdot(h, h).real > 0.5 * nw2:
+        return w, h
     h2 = B.conj().T @ w
     w = w - B @ h2
     return w, h + h2
