@@ -109,45 +109,6 @@ __global__ void k_dotc_multi_partial(int64_t n, int nv, const dcplx* __restrict_
   }
 }
 
-// One pass over w and up to CH basis vectors: per-block partials of conj(V_j) . w
-// (re, im) for j < nv and, if requested, of ||w||^2.  Deterministic block reduction.
-template <int CH>
-__global__ void __launch_bounds__(256) k_dotc_multi_norm_partial(int64_t n, int nv, const dcplx* __restrict__ V,
-                                                                 int64_t ldv, const dcplx* __restrict__ w,
-                                                                 double* __restrict__ part, int64_t ldp,
-                                                                 int with_norm) {
-  constexpr int NVAL = 2 * CH + 1;
-  __shared__ double sh[8][NVAL];
-  double acc[NVAL];
-#pragma unroll
-  for (int j = 0; j < NVAL; ++j) acc[j] = 0.0;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const dcplx wi = w[i];
-    if (with_norm) acc[2 * CH] = fma(wi.x, wi.x, fma(wi.y, wi.y, acc[2 * CH]));
-#pragma unroll
-    for (int j = 0; j < CH; ++j) {
-      if (j < nv) {
-        const dcplx v = V[i + ldv * j];
-        acc[2 * j] = fma(v.x, wi.x, fma(v.y, wi.y, acc[2 * j]));
-        acc[2 * j + 1] = fma(v.x, wi.y, fma(-v.y, wi.x, acc[2 * j + 1]));
-      }
-    }
-  }
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-  for (int j = 0; j < NVAL; ++j) {
-    double v = acc[j];
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if (lane == 0) sh[wid][j] = v;
-  }
-  __syncthreads();
-  for (int j = threadIdx.x; j < NVAL; j += blockDim.x) {
-    double t = 0.0;
-    for (int q = 0; q < 8; ++q) t += sh[q][j];
-    part[blockIdx.x + ldp * j] = t;
-  }
-}
-
 struct CoefPack {
   double2 c[32];
 };
@@ -401,33 +362,33 @@ cplx zdotc(Context* ctx, int64_t n, const dcplx* x, const dcplx* y) {
 }
 
 double zdotc_multi_norm(Context* ctx, int64_t n, int nv, const dcplx* V, int64_t ldv, const dcplx* w, cplx* h_host) {
-  constexpr int CH = 8;
-  constexpr int NVAL = 2 * CH + 1;
-  const int nb = std::min(red_blocks(n), 592);
-  const int nchunks = std::max(1, (nv + CH - 1) / CH);
-  DevBuf& red = ctx->buf("red_multi", (size_t)nb * NVAL * nchunks * sizeof(double));
-  DevBuf& out = ctx->buf("red_multi_out", (size_t)NVAL * nchunks * sizeof(double));
-  ScopedTimer t(ctx, "orth", (double)n * 16 * (nv + nchunks));
-  for (int c = 0; c < nchunks; ++c) {
-    const int nvc = std::max(0, std::min(CH, nv - c * CH));
-    k_dotc_multi_norm_partial<CH><<<nb, 256, 0, ctx->stream>>>(n, nvc, V + ldv * (int64_t)(c * CH), ldv, w,
-                                                               red.d() + (size_t)nb * NVAL * c, nb, c == 0 ? 1 : 0);
-    check_launch(ctx);
-  }
-  k_final_sum<<<1, kRedThreads, 0, ctx->stream>>>(nb, NVAL * nchunks, red.d(), nb, out.d());
-  check_launch(ctx);
-  std::vector<double> hv((size_t)NVAL * nchunks);
-  download(ctx, hv.data(), out.d(), hv.size() * sizeof(double));
-  for (int j = 0; j < nv; ++j) {
-    const int c = j / CH, jj = j % CH;
-    h_host[j] = cplx(hv[(size_t)NVAL * c + 2 * jj], hv[(size_t)NVAL * c + 2 * jj + 1]);
-  }
-  return std::sqrt(std::max(hv[2 * CH], 0.0));
+  // chunks of 8 basis vectors per pass (high occupancy beats re-reading w), then ||w||
+  if (nv > 0) zdotc_multi(ctx, n, nv, V, ldv, w, h_host);
+  return dznrm2(ctx, n, w);
 }
 
 void zdotc_multi(Context* ctx, int64_t n, int nv, const dcplx* V, int64_t ldv, const dcplx* w, cplx* h_host) {
   if (nv <= 0) return;
-  zdotc_multi_norm(ctx, n, nv, V, ldv, w, h_host);
+  int nb = std::min(red_blocks(n), 592);
+  constexpr int CH = 8;
+  int nchunks = (nv + CH - 1) / CH;
+  DevBuf& red = ctx->buf("red_multi", (size_t)nb * 2 * CH * nchunks * sizeof(double));
+  DevBuf& out = ctx->buf("red_multi_out", (size_t)2 * CH * nchunks * sizeof(double));
+  ScopedTimer t(ctx, "orth", (double)n * 16 * (nv + 1));
+  for (int c = 0; c < nchunks; ++c) {
+    int nvc = std::min(CH, nv - c * CH);
+    k_dotc_multi_partial<CH><<<nb, kRedThreads, 0, ctx->stream>>>(n, nvc, V + ldv * (int64_t)(c * CH), ldv, w,
+                                                                  red.d() + (size_t)nb * 2 * CH * c, nb);
+    check_launch(ctx);
+  }
+  k_final_sum<<<1, kRedThreads, 0, ctx->stream>>>(nb, 2 * CH * nchunks, red.d(), nb, out.d());
+  check_launch(ctx);
+  std::vector<double> hv(2 * CH * nchunks);
+  download(ctx, hv.data(), out.d(), hv.size() * sizeof(double));
+  for (int j = 0; j < nv; ++j) {
+    int c = j / CH, jj = j % CH;
+    h_host[j] = cplx(hv[2 * CH * c + 2 * jj], hv[2 * CH * c + 2 * jj + 1]);
+  }
 }
 
 static void gemv_common(Context* ctx, int64_t n, int nv, const dcplx* V, int64_t ldv, const cplx* coef, dcplx* w,
@@ -447,6 +408,7 @@ static void gemv_common(Context* ctx, int64_t n, int nv, const dcplx* V, int64_t
     if (cnt == 0) break;
   }
 }
+
 void zgemv_acc(Context* ctx, int64_t n, int nv, const dcplx* V, int64_t ldv, const cplx* coef, dcplx* w) {
   if (nv <= 0) return;
   gemv_common(ctx, n, nv, V, ldv, coef, w, 0);
