@@ -117,7 +117,9 @@ int imps_ctx_profile_reset(imps_ctx* ctx);
 int imps_ctx_profile_classes(imps_ctx* ctx, const char* csv);
 /* Every kernel class seen so far as text lines "class[@call-site] launches total_ms work". */
 int imps_ctx_profile_dump(imps_ctx* ctx, char* buf, int64_t len);
-/* counters[0..4] = AC applies, C applies, pushes, GEMM launches, all kernel launches */
+/* counters[0..7] (8 entries) = AC applies, C applies, pushes, GEMM launches, all kernel launches,
+ * QRpos/LQpos factorizations, real flops of all complex GEMMs (8 M N K each), real flops of
+ * the QR factorizations */
 int imps_ctx_counters(imps_ctx* ctx, int64_t* counters);
 
 /* -------------------------------------------------------------------- MPO */

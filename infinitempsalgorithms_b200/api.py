@@ -156,9 +156,10 @@ class Context:
         return out
 
     def counters(self):
-        arr = (C.c_int64 * 5)()
+        arr = (C.c_int64 * 8)()
         check(self.lib.imps_ctx_counters(self.h, arr), self.h)
-        return dict(ac_apply=arr[0], c_apply=arr[1], push=arr[2], gemm=arr[3], kernels=arr[4])
+        return dict(ac_apply=arr[0], c_apply=arr[1], push=arr[2], gemm=arr[3], kernels=arr[4], qr=arr[5],
+                    gemm_flops=arr[6], qr_flops=arr[7])
 
     def close(self):
         """Destroy the context; device objects created on it are released first."""

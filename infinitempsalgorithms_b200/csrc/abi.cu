@@ -267,6 +267,9 @@ int imps_ctx_counters(imps_ctx* h, int64_t* c) {
   c[2] = h->c.n_push;
   c[3] = h->c.n_gemm;
   c[4] = h->c.n_kernels;
+  c[5] = h->c.n_qr;
+  c[6] = (int64_t)h->c.gemm_flops;
+  c[7] = (int64_t)h->c.qr_flops;
   return IMPS_OK;
 }
 

@@ -127,7 +127,9 @@ struct Context {
   double pending_flops_dummy = 0;
   std::vector<double> pending_flops;
   // counters
-  int64_t n_ac_apply = 0, n_c_apply = 0, n_push = 0, n_gemm = 0, n_kernels = 0;
+  int64_t n_ac_apply = 0, n_c_apply = 0, n_push = 0, n_gemm = 0, n_kernels = 0, n_qr = 0;
+  double gemm_flops = 0.0;
+  double qr_flops = 0.0;    // real flops of the Householder QRpos factorizations (geqrf + ungqr)  // real flops of every complex GEMM requested (8 M N K), either precision
   int num_sms = 148;
   // split-precision state
   double split_tol = 1e-10;            // accuracy requested by the running solver

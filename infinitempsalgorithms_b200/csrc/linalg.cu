@@ -30,8 +30,11 @@ __global__ void k_extract_r(int k, int n, const dcplx* __restrict__ A, int64_t l
 
 void qrpos(Context* ctx, int m, int n, const dcplx* M, int64_t ldm, dcplx* Q, dcplx* R) {
   IMPS_REQUIRE(m > 0 && n > 0, IMPS_INVALID_ARG, "qrpos: empty matrix");
+  ctx->n_qr++;
   const int k = std::min(m, n);
-  ScopedTimer t(ctx, "qr", 8.0 * (2.0 * m * (double)n * k - 2.0 / 3.0 * k * (double)k * k) * 2.0);
+  const double qf = 8.0 * (2.0 * m * (double)n * k - 2.0 / 3.0 * k * (double)k * k) * 2.0;
+  ctx->qr_flops += qf;
+  ScopedTimer t(ctx, "qr", qf);
   DevBuf& Abuf = ctx->buf("qr_a", (size_t)m * n * sizeof(dcplx));
   DevBuf& tau = ctx->buf("qr_tau", (size_t)k * sizeof(dcplx));
   DevBuf& ph = ctx->buf("qr_ph", (size_t)k * sizeof(dcplx));

@@ -223,6 +223,7 @@ static std::shared_ptr<SplitOperand> get_split(Context* ctx, int side, Op op, in
 void zgemm(Context* ctx, Op opA, Op opB, int M, int N, int K, cplx alpha, const dcplx* A, int64_t lda,
            int64_t strideA, const dcplx* B, int64_t ldb, int64_t strideB, cplx beta, dcplx* C, int64_t ldc,
            int64_t strideC, int batch, bool allow_split) {
+  ctx->gemm_flops += 8.0 * (double)M * (double)N * (double)K * (double)batch;
   const int s = active_slices(ctx);
   const bool split = s > 0 && allow_split && opA != OP_T && opB != OP_T && alpha.imag() == 0.0 &&
                      (beta == cplx(0.0, 0.0) || beta == cplx(1.0, 0.0)) && M >= 64 && N >= 64 && K >= 32 &&

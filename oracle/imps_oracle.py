@@ -666,7 +666,7 @@ def push_slice_left(L, Wl, A):
     """``_push_slice_left`` (``envs.jl:104-107``): ``sum conj(A[a,u,a']) L[a,b] Wl[u,d] A[b,d,b']``."""
     Dl, d, Dr = A.shape
     Y = freshape(L @ freshape(A, (Dl, d * Dr)), (Dl, d, Dr))
-    Z = np.einsum("ud,adb->aub", Wl, Y)
+    Z = np.einsum("ud,adb->aub", Wl, Y, optimize=True)
     return np.asfortranarray(freshape(A, (Dl * d, Dr)).conj().T @ freshape(np.asfortranarray(Z), (Dl * d, Dr)))
 
 
@@ -674,7 +674,7 @@ def push_slice_right(R, Wl, A):
     """``_push_slice_right`` (``envs.jl:111-114``): ``sum A[a',d,a] R[a,b] Wl[u,d] conj(A[b',u,b])``."""
     Dl, d, Dr = A.shape
     Y = freshape(freshape(A, (Dl * d, Dr)) @ R, (Dl, d, Dr))
-    Z = np.einsum("ud,adb->aub", Wl, Y)
+    Z = np.einsum("ud,adb->aub", Wl, Y, optimize=True)
     return np.asfortranarray(freshape(np.asfortranarray(Z), (Dl, d * Dr)) @ freshape(A, (Dl, d * Dr)).conj().T)
 
 
@@ -684,7 +684,7 @@ def push_mpo_left(L, W, A):
     Dl, d, Dr = A.shape
     m, n = W.shape[0], W.shape[2]
     Y = freshape(freshape(L, (Dl * m, Dl)) @ freshape(A, (Dl, d * Dr)), (Dl, m, d, Dr))
-    Z = np.einsum("iujd,aidb->aujb", W, Y)
+    Z = np.einsum("iujd,aidb->aujb", W, Y, optimize=True)
     out = freshape(A, (Dl * d, Dr)).conj().T @ freshape(np.asfortranarray(Z), (Dl * d, n * Dr))
     return np.asfortranarray(freshape(out, (Dr, n, Dr)))
 
@@ -695,7 +695,7 @@ def push_mpo_right(R, W, A):
     Dl, d, Dr = A.shape
     m, n = W.shape[0], W.shape[2]
     Y = freshape(freshape(A, (Dl * d, Dr)) @ freshape(R, (Dr, n * Dr)), (Dl, d, n, Dr))
-    Z = np.einsum("iujd,adjb->aiub", W, Y)
+    Z = np.einsum("iujd,adjb->aiub", W, Y, optimize=True)
     out = freshape(np.asfortranarray(Z), (Dl * m, d * Dr)) @ freshape(A, (Dl, d * Dr)).conj().T
     return np.asfortranarray(freshape(out, (Dl, m, Dl)))
 
@@ -1123,7 +1123,7 @@ def ac_apply(GL, W, GR, x):
     Dl, d, Dr = x.shape
     m, n = W.shape[0], W.shape[2]
     T1 = freshape(freshape(GL, (Dl * m, Dl)) @ freshape(x, (Dl, d * Dr)), (Dl, m, d, Dr))
-    T2 = np.asfortranarray(np.einsum("iujs,bisc->bucj", W, T1))
+    T2 = np.asfortranarray(np.einsum("iujs,bisc->bucj", W, T1, optimize=True))
     y = freshape(T2, (Dl * d, Dr * n)) @ freshape(GR, (Dr * n, GR.shape[2]))
     return np.asfortranarray(freshape(y, (Dl, d, GR.shape[2])))
 
