@@ -48,9 +48,11 @@ def parse():
                         "residual (the mixed-precision form); fp64: the plain FP64 pipeline")
     p.add_argument("--nslices", type=int, default=0, help="int8 slices (0 = adaptive to the solver tolerance)")
     p.add_argument("--D", type=int, default=WORKLOAD["D"])
-    p.add_argument("--mode", default="vumps", choices=["vumps", "heff", "converge"],
+    p.add_argument("--mode", default="vumps", choices=["vumps", "heff", "converge", "tdvp"],
                    help="vumps: one VUMPS iteration per step; heff: one AC Heff apply per step; "
-                        "converge: VUMPS to convergence in FP64 and split precision from the same start")
+                        "converge: VUMPS to convergence in FP64 and split precision from the same start; "
+                        "tdvp: TFIM quench, TDVP in FP64 and split precision from one ground state")
+    p.add_argument("--tdvp-steps", type=int, default=200)
     p.add_argument("--model", default="hubbard", choices=["tfim", "xxz", "hubbard"])
     p.add_argument("--N", type=int, default=None)
     p.add_argument("--h", type=float, default=1.0, help="TFIM field")
@@ -206,6 +208,10 @@ def run_ours(args, world, rank, local):
         it += 1
         info = step(it, eps)
         eps = info.galerkin
+    # snapshot of the warmed-up state and environments: the end-to-end leg replays
+    # exactly the timed iterations from here
+    snap = snapshot(ctx, psi, envs) if not args.no_e2e else None
+    it0, eps0 = it, eps
     torch.cuda.synchronize()
     barrier(world)
     clocks = Clocks(local)
@@ -304,7 +310,8 @@ def run_ours(args, world, rank, local):
     result["heff_tflops"] = ac_flops(D, 4, 6) / (ms_ac / 1e3) / 1e12
     result["clocks"] = clk
     if not args.no_e2e:
-        result["e2e"] = run_e2e(args, ctx, psi, envs, H, it, eps, world)
+        restore(ctx, psi, envs, snap)
+        result["e2e"] = run_e2e(args, ctx, psi, envs, H, it0, eps0, world)
     return result, ctx, psi, envs, H
 
 
@@ -405,10 +412,94 @@ def run_converge(args, world, rank, local):
     return res
 
 
+def run_tdvp(args, world, rank, local):
+    """TDVP quench: FP64 VUMPS ground state of the TFIM at J=1, h=0.5 (bond D, seed 4),
+    then single-site TDVP under h=1.5 with dt = -0.01i for --tdvp-steps steps, once in
+    FP64 and once in split precision from the same ground state.  Reports TDVP
+    steps/s of each, <sigma_x>(t) and <sigma_z>(t) of both, the largest
+    difference between them, and each run's energy drift |E(t) - E(0)|."""
+    import torch
+    import infinitempsalgorithms_b200 as imps
+    from infinitempsalgorithms_b200 import _lib as L
+    torch.cuda.set_device(local)
+    J, h0, h1, dt = 1.0, 0.5, 1.5, -0.01j
+    D = args.D
+    H0, H1 = imps.tfim_hamiltonian(J, h0), imps.tfim_hamiltonian(J, h1)
+    sx, sz = imps.sigma("x"), imps.sigma("z")
+    ctx = imps.Context(local)
+    t0 = time.perf_counter()
+    psi0 = imps.CanonicalIMPS.from_sites(imps.random_site_tensors([2], D, 4), ctx=ctx)
+    gs, genvs, ginfo = imps.find_groundstate(psi0, H0, imps.VUMPS(D=D, maxiter=args.maxiter, tol=args.tol))
+    gs_s = time.perf_counter() - t0
+    snap = {f: gs.get(f, 0) for f in (L.IMPS_AL, L.IMPS_AR, L.IMPS_C, L.IMPS_AC)}
+    e_gs = imps.expectationvalue(gs, H0, genvs).real
+    ctx.close()
+    runs = {}
+    for prec in ("fp64", "split"):
+        c = imps.Context(local)
+        if prec == "split":
+            c.set_precision(L.IMPS_PREC_SPLIT_I8, args.nslices)
+        psi = imps.CanonicalIMPS(c, [2], [D])
+        for f, a in snap.items():
+            psi.set(f, 0, a)
+        envs = imps.DMRGCache(psi, H1)
+        E0 = imps.expectationvalue(psi, H1, envs).real
+        xs, zs, es = [imps.expectationvalue(psi, (1, sx)).real], [imps.expectationvalue(psi, (1, sz)).real], [E0]
+        t_steps = 0.0
+        for k in range(args.tdvp_steps):
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            psi, envs = imps.timestep(psi, H1, dt, imps.TDVP(), envs)
+            c.synchronize()
+            t_steps += time.perf_counter() - t1
+            xs.append(imps.expectationvalue(psi, (1, sx)).real)
+            zs.append(imps.expectationvalue(psi, (1, sz)).real)
+            es.append(imps.expectationvalue(psi, H1, envs).real)
+        runs[prec] = {"steps_per_s": args.tdvp_steps / t_steps, "s_per_step": t_steps / args.tdvp_steps,
+                      "energy_drift_max": float(np.max(np.abs(np.array(es) - E0))), "sx": xs, "sz": zs}
+        c.close()
+    dsx = float(np.max(np.abs(np.array(runs["split"]["sx"]) - np.array(runs["fp64"]["sx"]))))
+    dsz = float(np.max(np.abs(np.array(runs["split"]["sz"]) - np.array(runs["fp64"]["sz"]))))
+    every = max(1, args.tdvp_steps // 20)
+    for prec in runs:
+        runs[prec]["sx"] = [round(v, 12) for v in runs[prec]["sx"][::every]]
+        runs[prec]["sz"] = [round(v, 12) for v in runs[prec]["sz"][::every]]
+    return {"metric": f"TDVP steps/s (TFIM quench h=0.5->1.5, D={D}, dt=0.01)", "value": runs["split"]["steps_per_s"],
+            "unit": "step/s", "higher_is_better": True, "n_gpus": world,
+            "config": {"workload": "tdvp_quench_tfim", "J": J, "h0": h0, "h1": h1, "dt": "-0.01i", "D": D,
+                       "steps": args.tdvp_steps, "seed": 4, "gs_tol": args.tol, "nslices": args.nslices or "adaptive"},
+            "ground_state": {"iterations": ginfo.niter, "galerkin": ginfo.itererr, "energy_per_site": e_gs,
+                             "wall_s": gs_s},
+            "fp64": runs["fp64"], "split": runs["split"], "max_abs_dsx": dsx, "max_abs_dsz": dsz,
+            "sample_every_steps": every}
+
+
+def snapshot(ctx, psi, envs):
+    """Host copies of the state tensors and the environments (used to replay iterations)."""
+    from infinitempsalgorithms_b200 import _lib as L
+    st = {(f, l): psi.get(f, l) for l in range(psi.N) for f in (L.IMPS_AL, L.IMPS_AR, L.IMPS_C, L.IMPS_AC)}
+    ev = {}
+    for l in range(psi.N):
+        for side in (0, 1):
+            a = envs.leftenv(l + 1) if side == 0 else envs.rightenv(l + 1)
+            ev[(side, l)] = np.asfortranarray(a)
+    return st, ev
+
+
+def restore(ctx, psi, envs, snap):
+    from infinitempsalgorithms_b200 import _lib as L
+    st, ev = snap
+    for (f, l), a in st.items():
+        psi.set(f, l, a)
+    for (side, l), a in ev.items():
+        L.check(ctx.lib.imps_envs_set(envs.h, side, l, a.ctypes.data_as(L.DP)), ctx.h)
+
+
 def run_e2e(args, ctx, psi, envs, H, it, eps, world):
-    """Same metric through the C ABI with host buffers: each step uploads the
-    state (AL/AR/C/AC of both sites) from pinned host memory, runs
-    imps_vumps_iter, and downloads the new state and the energy."""
+    """Same metric through the C ABI with host buffers, replaying the timed
+    iterations from the warmed-up snapshot: each step uploads the state
+    (AL/AR/C/AC of both sites) from pinned host memory, runs imps_vumps_iter,
+    and downloads the new state and the energy."""
     import torch
     import ctypes as C
     from infinitempsalgorithms_b200 import _lib as L
@@ -542,6 +633,11 @@ def main():
         return
     if args.mode == "converge":
         res = run_converge(args, world, rank, local)
+        if rank == 0:
+            print(json.dumps(res))
+        return
+    if args.mode == "tdvp":
+        res = run_tdvp(args, world, rank, local)
         if rank == 0:
             print(json.dumps(res))
         return

@@ -244,6 +244,23 @@ int imps_energy(imps_envs* envs, const imps_mpo* mpo, imps_state* st, double* re
 /* expectationvalue(psi, (site,) => O) (src/observables/expval.jl:33-37); O is d x d. */
 int imps_local_expval(imps_state* st, int site, const double* O, double* re, double* im);
 
+/* ---------------------------------------------------------------- gradients */
+/* No counterpart in the reference (an extension for gradient-based iMPS
+ * optimisation).  Both use the environments in `envs`, which must be the fixed
+ * points for `st` and `mpo` (after imps_envs_build); the right environments are
+ * the solution of the adjoint of the left fixed-point system, so neither call
+ * iterates.  The state is taken as normalised (every canonical state is).
+ * G (host, interleaved complex, column-major (m, d, n, d)) = dE/dW[site]: the
+ * derivative of imps_energy's E with respect to each entry of the site's dense
+ * MPO tensor; the two identity blocks of the Schur form (level 1 -> 1 and
+ * m -> n) are returned as zero.  dE/dtheta for a coupling theta is
+ * sum(dW/dtheta * G) over the sites. */
+int imps_energy_grad_mpo(imps_envs* envs, const imps_mpo* mpo, imps_state* st, int site, double* G);
+/* g (host, interleaved complex, (Dl, d, Dr)) = dE/dconj(AL[site]) of the normalised
+ * energy of the uniform MPS generated by AL: (H_AC(AC) - lambda AC) C[site]^H with
+ * lambda = <AC|H_AC|AC>/<AC|AC>.  A real direction X changes E by 2 Re <g, X>. */
+int imps_energy_grad_al(imps_envs* envs, const imps_mpo* mpo, imps_state* st, int site, double* g);
+
 /* -------------------------------------------------------------- algorithms */
 /* localupdate_step! (vumps.jl:241-253): per site AC and C eigensolves + regauge!,
  * candidate ALs written into st->AL. */

@@ -124,6 +124,8 @@ _SIGS = {
     "imps_galerkin": (I32, [P, P, P, DP]),
     "imps_energy": (I32, [P, P, P, DP, DP]),
     "imps_local_expval": (I32, [P, I32, DP, DP, DP]),
+    "imps_energy_grad_mpo": (I32, [P, P, P, I32, DP]),
+    "imps_energy_grad_al": (I32, [P, P, P, I32, DP]),
     "imps_vumps_localupdate": (I32, [P, P, P, D, I32, I32, I32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "imps_vumps_iter": (I32, [P, P, P, I32, D, C.POINTER(VumpsInfo)]),
     "imps_tdvp_step": (I32, [P, P, P, D, D, D, I32, I32, D, I32, C.POINTER(KrylovInfo)]),

@@ -28,6 +28,7 @@ __all__ = [
     "C_hamiltonian", "fixedpoint", "integrate", "regauge", "calc_galerkin", "expectationvalue", "VUMPS",
     "IDMRG", "TDVP", "IterativeConvergenceInfo", "find_groundstate", "timestep", "time_evolve", "linsolve",
     "qrpos", "lqpos", "push_env_left", "push_env_right", "push_mpo_left", "push_mpo_right",
+    "energy_gradient_mpo", "energy_gradient_AL", "coupling_gradient", "rrule_energy",
 ]
 
 
@@ -745,6 +746,62 @@ def expectationvalue(psi: CanonicalIMPS, O=None, envs: Optional[DMRGCache] = Non
         check(ctx.lib.imps_local_expval(psi.h, (sites[0] - 1) % psi.N, dptr(op), C.byref(re), C.byref(im)), ctx.h)
         return complex(re.value, im.value)
     raise TypeError("unsupported operator")
+
+
+# ---------------------------------------------------------------------------
+# Energy gradients (no counterpart in the reference: an extension for
+# gradient-based iMPS optimisation; the right environments are the adjoint
+# solution of the left fixed-point system, so nothing iterates)
+# ---------------------------------------------------------------------------
+def energy_gradient_mpo(psi: CanonicalIMPS, H: SparseIMPO, envs: Optional[DMRGCache] = None) -> List[np.ndarray]:
+    """``[dE/dW_1, ..., dE/dW_N]``: derivative of ``expectationvalue(psi, H, envs)``
+    with respect to every entry of each site's dense MPO tensor (shape (m, d, n, d)).
+    The identity blocks of the Schur form come back as zero."""
+    ctx = psi.ctx
+    envs = envs or DMRGCache(psi, H)
+    out = []
+    for l in range(psi.N):
+        W = H[l + 1]
+        G = np.zeros(W.shape, complex, order="F")
+        check(ctx.lib.imps_energy_grad_mpo(envs.h, H.handle(ctx), psi.h, l, dptr(G)), ctx.h)
+        out.append(G)
+    return out
+
+
+def energy_gradient_AL(psi: CanonicalIMPS, H: SparseIMPO, envs: Optional[DMRGCache] = None) -> List[np.ndarray]:
+    """``[dE/dconj(AL_1), ...]``: Wirtinger gradient of the normalised energy of the
+    uniform MPS generated by ``AL``; a direction ``X`` changes E by ``2 Re <g, X>``."""
+    ctx = psi.ctx
+    envs = envs or DMRGCache(psi, H)
+    out = []
+    for l in range(psi.N):
+        g = np.zeros(psi._shape(L.IMPS_AL, l), complex, order="F")
+        check(ctx.lib.imps_energy_grad_al(envs.h, H.handle(ctx), psi.h, l, dptr(g)), ctx.h)
+        out.append(g)
+    return out
+
+
+def coupling_gradient(psi: CanonicalIMPS, H: SparseIMPO, dW: Sequence[np.ndarray],
+                      envs: Optional[DMRGCache] = None) -> complex:
+    """``dE/dtheta`` for an MPO whose site tensors depend on a coupling theta with
+    derivatives ``dW[l] = dW_l/dtheta`` (E is linear in each W entry, so this is the
+    contraction of ``dW`` with ``energy_gradient_mpo``)."""
+    G = energy_gradient_mpo(psi, H, envs)
+    return complex(sum(np.sum(np.asarray(dW[l % len(dW)]) * G[l]) for l in range(psi.N)))
+
+
+def rrule_energy(psi: CanonicalIMPS, H: SparseIMPO, envs: Optional[DMRGCache] = None):
+    """Reverse rule for ``expectationvalue(psi, H, envs)``: returns ``(E, pullback)``
+    with ``pullback(Ebar) -> (dW list, dAL list)`` (cotangents of the MPO tensors
+    and of the conjugated ``AL`` tensors for a real cotangent ``Ebar``)."""
+    envs = envs or DMRGCache(psi, H)
+    E = expectationvalue(psi, H, envs)
+    GW = energy_gradient_mpo(psi, H, envs)
+    GA = energy_gradient_AL(psi, H, envs)
+
+    def pullback(Ebar=1.0):
+        return [Ebar * g for g in GW], [Ebar * g for g in GA]
+    return E, pullback
 
 
 # ---------------------------------------------------------------------------

@@ -1,6 +1,7 @@
 // The extern "C" boundary (include/imps_b200.h).  Every entry point catches
 // exceptions and maps them to IMPS_* status codes; the message is kept in the
 // context (imps_ctx_last_error) and in a thread-local fallback.
+#include <cstdlib>
 #include <cstring>
 #include <string>
 
@@ -118,6 +119,7 @@ int imps_ctx_create(int device, imps_ctx** out) {
     IMPS_SOLVER(cusolverDnSetStream(c.solver, c.stream));
     IMPS_CUDA(cudaMalloc((void**)&c.dev_info, sizeof(int) * 4));
     cudaDeviceGetAttribute(&c.num_sms, cudaDevAttrMultiProcessorCount, device);
+    if (const char* e = std::getenv("IMPS_FP64_ENGINE")) c.fp64_engine = std::atoi(e) == 1 ? 1 : 0;
     return IMPS_OK;
   });
   if (r != IMPS_OK) {
@@ -846,6 +848,29 @@ int imps_local_expval(imps_state* st, int site, const double* O, double* re, dou
     imps::cplx v = imps::local_expval(st->ctx, st, site, hc(O));
     if (re) *re = v.real();
     if (im) *im = v.imag();
+    return IMPS_OK;
+  });
+}
+
+// ------------------------------------------------------------------ gradients
+int imps_energy_grad_mpo(imps_envs* E, const imps_mpo* mpo, imps_state* st, int site, double* G) {
+  if (!E || !mpo || !st || !G) return IMPS_INVALID_ARG;
+  return guard(E->ctx, [&] {
+    IMPS_REQUIRE(site >= 0 && site < st->N && st->N == E->N, IMPS_INVALID_ARG, "site index out of range");
+    imps::energy_grad_mpo(E->ctx, E, mpo, st, site, reinterpret_cast<imps::cplx*>(G));
+    return IMPS_OK;
+  });
+}
+
+int imps_energy_grad_al(imps_envs* E, const imps_mpo* mpo, imps_state* st, int site, double* g) {
+  if (!E || !mpo || !st || !g) return IMPS_INVALID_ARG;
+  return guard(E->ctx, [&] {
+    IMPS_REQUIRE(site >= 0 && site < st->N && st->N == E->N, IMPS_INVALID_ARG, "site index out of range");
+    imps::Context* ctx = E->ctx;
+    const size_t n = st->site_elems(site);
+    imps::DevBuf& gd = ctx->buf("grad_al_out", n * sizeof(imps::dcplx));
+    imps::energy_grad_al(ctx, E, mpo, st, site, gd.z());
+    imps::download(ctx, g, gd.ptr, n * sizeof(imps::dcplx));
     return IMPS_OK;
   });
 }

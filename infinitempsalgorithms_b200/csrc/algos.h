@@ -7,6 +7,10 @@ namespace imps {
 double galerkin(Context* ctx, imps_envs* E, const imps_mpo* H, const imps_state* st);
 cplx energy(Context* ctx, imps_envs* E, const imps_mpo* H, imps_state* st);
 cplx local_expval(Context* ctx, imps_state* st, int site, const cplx* O);
+// energy gradients (grad.cu): dE/dW[site] into G_host (m, d, n, d); dE/dconj(AL[site]) into g (device)
+void energy_grad_mpo(Context* ctx, const imps_envs* E, const imps_mpo* H, const imps_state* st, int site,
+                     cplx* G_host);
+void energy_grad_al(Context* ctx, const imps_envs* E, const imps_mpo* H, const imps_state* st, int site, dcplx* g);
 KrylovResult eigsolve_ac(Context* ctx, imps_envs* E, const imps_mpo* H, int site, const dcplx* x0, dcplx* x,
                          double tol, int kdim, int maxiter, bool eager);
 KrylovResult eigsolve_c(Context* ctx, imps_envs* E, int site, const dcplx* x0, dcplx* x, double tol, int kdim,

@@ -13,18 +13,25 @@
 // epilogue adds r_i c_j 2^-7(d+2) acc to the FP64 output.  Truncation error per
 // element is below 2^-7s of the row/column scale.
 //
-// GEMM kernel: persistent, one CTA per SM, warp-specialised:
-//   warp 0: TMA producer (cp.async.bulk.tensor, 128B swizzle, 4-stage ring)
-//   warp 1: TMEM allocator + single-thread tcgen05.mma issuer (M=128, N=256, K=32)
-//   warps 2-5: epilogue, tcgen05.ld 32x32b from a double-buffered accumulator
+// GEMM kernel: persistent, one CTA per SM, warp-specialised, 128 x 128 output tiles:
+//   warp 0: TMA producer (cp.async.bulk.tensor, 128B swizzle, 6-stage ring of
+//           16 KB A + 16 KB B stages)
+//   warp 1: TMEM allocator + single-thread tcgen05.mma issuer (M=128, N=128, K=32);
+//           every slice diagonal of a tile accumulates in its own int32 TMEM slot
+//           (4 slots x 128 columns)
+//   warps 2-9: epilogue, tcgen05.ld 32x32b, two warps per TMEM lane quarter; each
+//           thread keeps the FP64 partial sums of its row over all diagonals in
+//           registers and writes the tile once
 // Every mbarrier wait is bounded (~1 s of clock64); on expiry the kernel sets an
 // error flag, drains and returns, and the host raises IMPS_TIMEOUT.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 
 #include "imps_internal.h"
 #include "split_gemm.h"
@@ -39,7 +46,7 @@ constexpr int STAGES = 6;
 constexpr int NSLOT = 4;         // TMEM accumulator slots of BN columns (4 x 128 = 512)
 constexpr int EPI_WARPS = 8;     // two warps per TMEM lane quarter, each owning BN/2 columns
 constexpr int A_STAGE = BM * BKB;   // 16 KB
-constexpr int B_STAGE = BN * BKB;   // 32 KB
+constexpr int B_STAGE = BN * BKB;   // 16 KB
 constexpr int SMEM_TILES = STAGES * (A_STAGE + B_STAGE);
 constexpr int SMEM_BYTES = SMEM_TILES + 1024 /*align*/ + 256 /*barriers*/;
 constexpr int NTHREADS = 32 * (2 + EPI_WARPS);
@@ -523,7 +530,10 @@ __global__ void __launch_bounds__(256) k_split_b(int K, int N, const double2* __
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
+  // resolved once per process; contexts on several host threads may race here
+  static std::mutex mu;
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  std::lock_guard<std::mutex> lock(mu);
   if (!fn) {
     cudaDriverEntryPointQueryResult q;
     void* p = nullptr;
@@ -625,10 +635,12 @@ void split_gemm(Context* ctx, const SplitOperand& A, const SplitOperand& B, int 
                 dcplx* C, int64_t ldc) {
   IMPS_REQUIRE(A.K == B.K && A.Kp == B.Kp, IMPS_DIM_MISMATCH, "split_gemm: inner dimensions differ");
   IMPS_REQUIRE(s >= 1 && s <= A.s && s <= B.s && s <= 8, IMPS_INVALID_ARG, "split_gemm: bad slice count");
-  static bool attr = false;
-  if (!attr) {
+  // the shared-memory opt-in is per device; setting it again is harmless
+  static std::atomic<uint64_t> attr_devices{0};
+  const uint64_t bit = 1ull << (ctx->device & 63);
+  if (!(attr_devices.load() & bit)) {
     IMPS_CUDA(cudaFuncSetAttribute(k_gemm_i8, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
-    attr = true;
+    attr_devices.fetch_or(bit);
   }
   const CUtensorMap mapA = make_map(static_cast<const int8_t*>(A.data.ptr), A.Kp, A.Rp, A.s, BM);
   const CUtensorMap mapB = make_map(static_cast<const int8_t*>(B.data.ptr), B.Kp, B.Rp, B.s, BN);

@@ -109,6 +109,7 @@ struct Context {
   int precision = PREC_FP64;
   int nslices = 5;           // int8 slices per operand in split mode
   bool adaptive_slices = false;
+  int fp64_engine = 0;       // FP64 GEMM kernel: 0 = DMMA tensor cores, 1 = SIMT DFMA (env IMPS_FP64_ENGINE)
   std::string last_error;
   // named grow-only scratch buffers
   std::map<std::string, DevBuf> scratch;
@@ -306,6 +307,11 @@ cplx zdotc(Context* ctx, int64_t n, const dcplx* x, const dcplx* y);  // sum con
 void zdotc_multi(Context* ctx, int64_t n, int nv, const dcplx* V, int64_t ldv, const dcplx* w, cplx* h_host);
 // same, and returns ||w|| from the same pass over w
 double zdotc_multi_norm(Context* ctx, int64_t n, int nv, const dcplx* V, int64_t ldv, const dcplx* w, cplx* h_host);
+// One classical Gram-Schmidt projection w <- w - V h with h = V^H w, all on the device
+// and one host synchronisation: returns ||w_new||^2, writes h (host) and, if nw_old2
+// is given, ||w_old||^2.
+double proj_pass(Context* ctx, int64_t n, int nv, const dcplx* V, int64_t ldv, dcplx* w, cplx* h_host,
+                 double* nw_old2);
 // w += sum_j coef[j] V[:, j]
 void zgemv_acc(Context* ctx, int64_t n, int nv, const dcplx* V, int64_t ldv, const cplx* coef, dcplx* w);
 // y = sum_j coef[j] V[:, j]

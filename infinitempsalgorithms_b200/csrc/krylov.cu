@@ -18,28 +18,23 @@
 namespace imps {
 namespace {
 
-// Classical Gram-Schmidt with the DGKS criterion: w <- w - V h; a second pass runs
-// only if the first one removed more than 1 - 1/sqrt(2) of the norm of w.  Returns
-// the coefficients (host) and ||w|| after orthogonalisation.
+// Classical Gram-Schmidt with iterative refinement (KrylovKit's
+// ClassicalGramSchmidtIR, eta = 1/sqrt(2)): w <- w - V h; the projection is
+// repeated while it shrank ||w|| below eta times its previous value (at most three
+// passes).  Returns the accumulated coefficients (host) and the final ||w||.
 double cgs2(Context* ctx, int64_t n, int nv, const dcplx* V, dcplx* w, std::vector<cplx>& h) {
   h.assign(nv, cplx(0.0, 0.0));
   if (nv == 0) return dznrm2(ctx, n, w);
-  std::vector<cplx> h1(nv), neg(nv);
-  double nw = zdotc_multi_norm(ctx, n, nv, V, n, w, h1.data());
-  for (int pass = 0; pass < 2; ++pass) {
-    for (int j = 0; j < nv; ++j) {
-      neg[j] = -h1[j];
-      h[j] += h1[j];
-    }
-    zgemv_acc(ctx, n, nv, V, n, neg.data(), w);
-    if (pass == 1) break;
-    double nproj = 0.0;
-    for (int j = 0; j < nv; ++j) nproj += std::norm(h1[j]);
-    const double nrest2 = nw * nw - nproj;  // ||w - V h||^2 in exact arithmetic
-    if (nrest2 > 0.5 * nw * nw) return dznrm2(ctx, n, w);
-    nw = zdotc_multi_norm(ctx, n, nv, V, n, w, h1.data());
+  std::vector<cplx> h1(nv);
+  double nw0 = 0.0;
+  double nw1 = proj_pass(ctx, n, nv, V, n, w, h1.data(), &nw0);
+  for (int j = 0; j < nv; ++j) h[j] += h1[j];
+  for (int pass = 1; pass < 3 && nw1 < 0.5 * nw0; ++pass) {
+    nw0 = nw1;
+    nw1 = proj_pass(ctx, n, nv, V, n, w, h1.data(), nullptr);
+    for (int j = 0; j < nv; ++j) h[j] += h1[j];
   }
-  return dznrm2(ctx, n, w);
+  return std::sqrt(std::max(nw1, 0.0));
 }
 
 std::vector<cplx> herm_part(const std::vector<cplx>& H, int ldh, int m) {

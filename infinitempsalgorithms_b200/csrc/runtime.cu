@@ -109,6 +109,80 @@ __global__ void k_dotc_multi_partial(int64_t n, int nv, const dcplx* __restrict_
   }
 }
 
+// One block per column: out[c] = sum_i part[i + ld c] (same order as k_final_sum).
+__global__ void k_final_sum_cols(int nb, const double* __restrict__ part, int64_t ld, double* __restrict__ out) {
+  __shared__ double sh[kRedThreads / 32];
+  const int c = blockIdx.x;
+  double s = 0.0;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) s += part[i + ld * c];
+  double r = block_sum<kRedThreads>(s, sh);
+  if (threadIdx.x == 0) out[c] = r;
+}
+
+// Projection pass, step 1: partials of h_j = <V_j, w> for a chunk of up to CH
+// vectors (columns 2 j0 + 2 j, +1 of `part`) and, when norm_col >= 0, of ||w||^2.
+template <int CH>
+__global__ void k_proj_dots(int64_t n, int nv, const dcplx* __restrict__ V, int64_t ldv, const dcplx* __restrict__ w,
+                            double* __restrict__ part, int64_t ldp, int col0, int norm_col) {
+  __shared__ double sh[kRedThreads / 32];
+  double ar[CH], ai[CH], nn = 0.0;
+#pragma unroll
+  for (int j = 0; j < CH; ++j) { ar[j] = 0.0; ai[j] = 0.0; }
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const dcplx wi = w[i];
+    nn = fma(wi.x, wi.x, fma(wi.y, wi.y, nn));
+#pragma unroll
+    for (int j = 0; j < CH; ++j) {
+      if (j < nv) {
+        const dcplx p = cmulc(V[i + ldv * j], wi);
+        ar[j] += p.x;
+        ai[j] += p.y;
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < CH; ++j) {
+    if (j < nv) {
+      const double r = block_sum<kRedThreads>(ar[j], sh);
+      const double q = block_sum<kRedThreads>(ai[j], sh);
+      if (threadIdx.x == 0) {
+        part[blockIdx.x + ldp * (col0 + 2 * j)] = r;
+        part[blockIdx.x + ldp * (col0 + 2 * j + 1)] = q;
+      }
+    }
+  }
+  if (norm_col >= 0) {
+    const double r = block_sum<kRedThreads>(nn, sh);
+    if (threadIdx.x == 0) part[blockIdx.x + ldp * norm_col] = r;
+  }
+}
+
+// Projection pass, step 2: w -= sum_j h_j V_j for up to 32 vectors, h read from the
+// device (interleaved re/im at hdev[2 j0 ..]); on the last chunk also the partials
+// of the new ||w||^2 (one per block) go to `npart`.
+__global__ void k_proj_update(int64_t n, int nv, const dcplx* __restrict__ V, int64_t ldv,
+                              const double* __restrict__ hdev, dcplx* __restrict__ w, double* __restrict__ npart) {
+  __shared__ double2 c[32];
+  __shared__ double sh[kRedThreads / 32];
+  if (threadIdx.x < nv) c[threadIdx.x] = make_double2(-hdev[2 * threadIdx.x], -hdev[2 * threadIdx.x + 1]);
+  __syncthreads();
+  double nn = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    dcplx acc = w[i];
+    for (int j = 0; j < nv; ++j) {
+      const dcplx p = cmul(c[j], V[i + ldv * j]);
+      acc.x += p.x;
+      acc.y += p.y;
+    }
+    w[i] = acc;
+    nn = fma(acc.x, acc.x, fma(acc.y, acc.y, nn));
+  }
+  if (npart) {
+    const double r = block_sum<kRedThreads>(nn, sh);
+    if (threadIdx.x == 0) npart[blockIdx.x] = r;
+  }
+}
+
 struct CoefPack {
   double2 c[32];
 };
@@ -415,6 +489,49 @@ void zgemv_acc(Context* ctx, int64_t n, int nv, const dcplx* V, int64_t ldv, con
 }
 void zgemv_set(Context* ctx, int64_t n, int nv, const dcplx* V, int64_t ldv, const cplx* coef, dcplx* y) {
   gemv_common(ctx, n, nv, V, ldv, coef, y, 1);
+}
+
+double proj_pass(Context* ctx, int64_t n, int nv, const dcplx* V, int64_t ldv, dcplx* w, cplx* h_host,
+                 double* nw_old2) {
+  // columns of the partials: 2 nv dot columns, then ||w_old||^2, then ||w_new||^2
+  const int nb = std::min(red_blocks(n), 592);
+  constexpr int CH = 8;
+  const int ncol = 2 * nv + 2;
+  DevBuf& red = ctx->buf("proj_part", (size_t)nb * ncol * sizeof(double));
+  DevBuf& out = ctx->buf("proj_out", (size_t)ncol * sizeof(double));
+  ScopedTimer t(ctx, "orth", (double)n * 16 * (2 * nv + 3));
+  const int norm_col = nw_old2 ? 2 * nv : -1;
+  if (nv == 0 && nw_old2) {
+    k_proj_dots<CH><<<nb, kRedThreads, 0, ctx->stream>>>(n, 0, V, ldv, w, red.d(), nb, 0, norm_col);
+    check_launch(ctx);
+  }
+  for (int c0 = 0; c0 < nv; c0 += CH) {
+    const int nvc = std::min(CH, nv - c0);
+    k_proj_dots<CH><<<nb, kRedThreads, 0, ctx->stream>>>(n, nvc, V + ldv * (int64_t)c0, ldv, w, red.d(), nb, 2 * c0,
+                                                         c0 == 0 ? norm_col : -1);
+    check_launch(ctx);
+  }
+  const int ndots = 2 * nv + (nw_old2 ? 1 : 0);
+  if (ndots > 0) {
+    k_final_sum_cols<<<ndots, kRedThreads, 0, ctx->stream>>>(nb, red.d(), nb, out.d());
+    check_launch(ctx);
+  }
+  for (int c0 = 0; c0 < nv || (nv == 0 && c0 == 0); c0 += 32) {
+    const int cnt = std::min(32, nv - c0);
+    const bool last = c0 + 32 >= nv;
+    k_proj_update<<<nb, kRedThreads, 0, ctx->stream>>>(n, cnt, V + ldv * (int64_t)c0, ldv, out.d() + 2 * c0, w,
+                                                       last ? red.d() + (size_t)nb * (2 * nv + 1) : nullptr);
+    check_launch(ctx);
+    if (nv == 0) break;
+  }
+  k_final_sum_cols<<<1, kRedThreads, 0, ctx->stream>>>(nb, red.d() + (size_t)nb * (2 * nv + 1), nb,
+                                                       out.d() + 2 * nv + 1);
+  check_launch(ctx);
+  std::vector<double> hv(ncol);
+  download(ctx, hv.data(), out.d(), hv.size() * sizeof(double));
+  for (int j = 0; j < nv; ++j) h_host[j] = cplx(hv[2 * j], hv[2 * j + 1]);
+  if (nw_old2) *nw_old2 = hv[2 * nv];
+  return hv[2 * nv + 1];
 }
 
 void zconj_transpose(Context* ctx, int m, int n, const dcplx* X, int64_t ldx, dcplx* Y, int64_t ldy) {

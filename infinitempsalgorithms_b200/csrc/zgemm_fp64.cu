@@ -8,6 +8,7 @@
 #include "imps_internal.h"
 #include "split_gemm.h"
 
+#include <atomic>
 #include <cmath>
 
 namespace imps {
@@ -124,15 +125,183 @@ __global__ void __launch_bounds__(NT, 2)
   }
 }
 
+// ---------------------------------------------------------------------------
+// FP64 tensor-core variant: mma.sync m8n8k4 f64 (DMMA).  128 x 64 complex output
+// tile per CTA of 8 warps (4 x 2 warps of 32 x 32), K stage of 16 complex, a
+// 3-stage cp.async ring (zero-filled at the matrix edges).  A complex product is
+// four real DMMAs per 8 x 8 block: re += ar br - ai bi, im += ar bi + ai br; the
+// conjugate of an operand only flips the sign of its imaginary fragment.
+// Shared tiles are k-major rows of double2 with one element of padding.
+// ---------------------------------------------------------------------------
+namespace dm {
+constexpr int BM = 128, BN = 64, BK = 16, STAGES = 3, NT = 256;
+constexpr int LDA = BM + 1, LDB = BN + 1;
+constexpr int A_ELEMS = BK * LDA, B_ELEMS = BK * LDB;
+constexpr int SMEM = STAGES * (A_ELEMS + B_ELEMS) * 16;
+}  // namespace dm
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, int bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+template <int OPA, int OPB, bool BETA>
+__global__ void __launch_bounds__(dm::NT, 1)
+    k_zgemm_dmma(int M, int N, int K, double2 alpha, const double2* __restrict__ A, int64_t lda, int64_t sA,
+                 const double2* __restrict__ B, int64_t ldb, int64_t sB, double2 beta, double2* __restrict__ C,
+                 int64_t ldc, int64_t sC) {
+  extern __shared__ __align__(16) double2 smem_dm[];
+  double2* As = smem_dm;                      // [dm::STAGES][dm::BK][dm::LDA]
+  double2* Bs = smem_dm + dm::STAGES * dm::A_ELEMS;   // [dm::STAGES][dm::BK][dm::LDB]
+  const int bz = blockIdx.z;
+  A += sA * bz;
+  B += sB * bz;
+  C += sC * bz;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp & 3, wn = warp >> 2;  // warp tile origin (32 * wm, 32 * wn)
+  const int m0 = blockIdx.x * dm::BM, n0 = blockIdx.y * dm::BN;
+  const uint32_t sbase = static_cast<uint32_t>(__cvta_generic_to_shared(smem_dm));
+
+  auto issue = [&](int stage, int k0) {
+    // A tile: dm::BM x dm::BK complex, 4 per thread
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      int m, k;
+      if (OPA == OP_N) { m = tid & 127; k = (tid >> 7) + 2 * r; }
+      else { k = tid & 7; m = (tid >> 3) + 32 * r; }
+      const int gm = m0 + m, gk = k0 + k;
+      const bool ok = gm < M && gk < K;
+      const double2* src = ok ? ((OPA == OP_N) ? A + gm + lda * (int64_t)gk : A + gk + lda * (int64_t)gm) : A;
+      cp_async16(sbase + 16u * (stage * dm::A_ELEMS + k * dm::LDA + m), src, ok ? 16 : 0);
+    }
+    // B tile: dm::BK x dm::BN complex, 2 per thread
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      int n, k;
+      if (OPB == OP_N) { k = tid & 7; n = (tid >> 3) + 32 * r; }
+      else { n = tid & 63; k = (tid >> 6) + 4 * r; }
+      const int gn = n0 + n, gk = k0 + k;
+      const bool ok = gn < N && gk < K;
+      const double2* src = ok ? ((OPB == OP_N) ? B + gk + ldb * (int64_t)gn : B + gn + ldb * (int64_t)gk) : B;
+      cp_async16(sbase + 16u * (dm::STAGES * dm::A_ELEMS + stage * dm::B_ELEMS + k * dm::LDB + n), src, ok ? 16 : 0);
+    }
+  };
+
+  double cre[4][4][2], cim[4][4][2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) cre[i][j][0] = cre[i][j][1] = cim[i][j][0] = cim[i][j][1] = 0.0;
+
+  const int ktiles = (K + dm::BK - 1) / dm::BK;
+#pragma unroll
+  for (int st = 0; st < dm::STAGES - 1; ++st) {
+    if (st < ktiles) issue(st, st * dm::BK);
+    cp_async_commit();
+  }
+  const int fr = lane >> 2, fk = lane & 3;  // fragment row/col (A: row m, col k; B: col n, row k)
+  for (int kt = 0; kt < ktiles; ++kt) {
+    cp_async_wait<dm::STAGES - 2>();
+    __syncthreads();
+    {
+      const int nk = kt + dm::STAGES - 1;
+      if (nk < ktiles) issue(nk % dm::STAGES, nk * dm::BK);
+      cp_async_commit();
+    }
+    const double2* as = As + (kt % dm::STAGES) * dm::A_ELEMS;
+    const double2* bs = Bs + (kt % dm::STAGES) * dm::B_ELEMS;
+#pragma unroll
+    for (int kb = 0; kb < dm::BK; kb += 4) {
+      double ar[4], ai[4], nai[4], br[4], bi[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const double2 v = as[(kb + fk) * dm::LDA + 32 * wm + 8 * i + fr];
+        ar[i] = v.x;
+        ai[i] = (OPA == OP_C) ? -v.y : v.y;
+        nai[i] = -ai[i];
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const double2 v = bs[(kb + fk) * dm::LDB + 32 * wn + 8 * j + fr];
+        br[j] = v.x;
+        bi[j] = (OPB == OP_C) ? -v.y : v.y;
+      }
+      // the two updates of one accumulator are 32 MMAs apart
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          dmma(cre[i][j][0], cre[i][j][1], ar[i], br[j]);
+          dmma(cim[i][j][0], cim[i][j][1], ar[i], bi[j]);
+        }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          dmma(cre[i][j][0], cre[i][j][1], nai[i], bi[j]);
+          dmma(cim[i][j][0], cim[i][j][1], ai[i], br[j]);
+        }
+    }
+  }
+  cp_async_wait<0>();
+  // D fragment: row = lane >> 2, cols 2 (lane & 3) + {0, 1} of each 8 x 8 block
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int gm = m0 + 32 * wm + 8 * i + fr;
+    if (gm >= M) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int gn = n0 + 32 * wn + 8 * j + 2 * fk + e;
+        if (gn >= N) continue;
+        const double vr = cre[i][j][e], vi = cim[i][j][e];
+        double2 o = make_double2(alpha.x * vr - alpha.y * vi, alpha.x * vi + alpha.y * vr);
+        if (BETA) {
+          const double2 c = C[gm + ldc * (int64_t)gn];
+          o.x += beta.x * c.x - beta.y * c.y;
+          o.y += beta.x * c.y + beta.y * c.x;
+        }
+        C[gm + ldc * (int64_t)gn] = o;
+      }
+    }
+  }
+}
+
 template <int OPA, int OPB>
 void launch(Context* ctx, int M, int N, int K, double2 alpha, const dcplx* A, int64_t lda, int64_t sA,
             const dcplx* B, int64_t ldb, int64_t sB, double2 beta, dcplx* C, int64_t ldc, int64_t sC, int batch,
             bool use_beta) {
-  dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN, batch);
-  if (use_beta)
-    k_zgemm<OPA, OPB, true><<<grid, NT, 0, ctx->stream>>>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC);
-  else
-    k_zgemm<OPA, OPB, false><<<grid, NT, 0, ctx->stream>>>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC);
+  if (ctx->fp64_engine == 1) {
+    dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN, batch);
+    if (use_beta)
+      k_zgemm<OPA, OPB, true><<<grid, NT, 0, ctx->stream>>>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC);
+    else
+      k_zgemm<OPA, OPB, false><<<grid, NT, 0, ctx->stream>>>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc,
+                                                              sC);
+    return;
+  }
+  // the dynamic shared-memory opt-in is per device and per kernel instance; setting it
+  // twice (two host threads racing here) is harmless
+  static std::atomic<uint64_t> attr_set[2];
+  auto kern = use_beta ? k_zgemm_dmma<OPA, OPB, true> : k_zgemm_dmma<OPA, OPB, false>;
+  const uint64_t bit = 1ull << (ctx->device & 63);
+  std::atomic<uint64_t>& done = attr_set[use_beta ? 1 : 0];
+  if (!(done.load() & bit)) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, dm::SMEM);
+    if (e != cudaSuccess) throw Error(IMPS_CUDA_ERROR, std::string("zgemm smem opt-in: ") + cudaGetErrorString(e));
+    done.fetch_or(bit);
+  }
+  dim3 grid((M + dm::BM - 1) / dm::BM, (N + dm::BN - 1) / dm::BN, batch);
+  kern<<<grid, dm::NT, dm::SMEM, ctx->stream>>>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC);
 }
 
 }  // namespace
@@ -142,7 +311,7 @@ void zgemm_fp64(Context* ctx, Op opA, Op opB, int M, int N, int K, cplx alpha, c
                 int64_t strideC, int batch) {
   if (M <= 0 || N <= 0 || batch <= 0) return;
   IMPS_REQUIRE(batch <= 65535, IMPS_INVALID_ARG, "zgemm: batch too large");
-  IMPS_REQUIRE((N + BN - 1) / BN <= 65535, IMPS_INVALID_ARG, "zgemm: N too large");
+  IMPS_REQUIRE((N + dm::BN - 1) / dm::BN <= 65535, IMPS_INVALID_ARG, "zgemm: N too large");
   if (K <= 0) {
     // C = beta C
     for (int b = 0; b < batch; ++b) {

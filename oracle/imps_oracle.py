@@ -43,7 +43,7 @@ from typing import Callable, List, Optional, Sequence
 import numpy as np
 
 __all__ = [
-    "freshape", "fzeros", "C128", "Defaults", "DynamicTol", "alg_eigsolve", "alg_gauge",
+    "freshape", "fzeros", "C128", "energy_grad_mpo", "energy_grad_al", "Defaults", "DynamicTol", "alg_eigsolve", "alg_gauge",
     "alg_environments", "alg_expsolve", "canonical_from_AL", "canonical_from_sites",
     "canonical_from_AL_keepAL", "_mulAL", "_mulCA", "hubbard_operators", "updatetol", "sigma", "spin", "mpohamiltonian",
     "SchurMPO", "tfim_hamiltonian", "heisenberg_hamiltonian", "hubbard_hamiltonian",
@@ -344,19 +344,25 @@ class KrylovInfo:
 
 
 def _cgs2(V: List[np.ndarray], w: np.ndarray):
-    """Classical Gram-Schmidt with the DGKS criterion: a second pass only when the
-    first one removed more than 1 - 1/sqrt(2) of ||w|| (||w - V h||^2 <= ||w||^2 / 2)."""
+    """Classical Gram-Schmidt with iterative refinement (KrylovKit's
+    ``ClassicalGramSchmidtIR`` with eta = 1/sqrt(2)): the projection is repeated
+    while it shrank ||w|| below eta times its previous value, at most three passes."""
     if not V:
         return w, np.zeros(0, dtype=C128)
     B = np.stack(V, axis=1)
-    nw2 = np.vdot(w, w).real
+    nw0 = np.vdot(w, w).real
     h = B.conj().T @ w
     w = w - B @ h
-    if nw2 - np.vdot(h, h).real > 0.5 * nw2:
-        return w, h
-    h2 = B.conj().T @ w
-    w = w - B @ h2
-    return w, h + h2
+    nw1 = np.vdot(w, w).real
+    passes = 1
+    while passes < 3 and nw1 < 0.5 * nw0:
+        nw0 = nw1
+        h2 = B.conj().T @ w
+        w = w - B @ h2
+        h = h + h2
+        nw1 = np.vdot(w, w).real
+        passes += 1
+    return w, h
 
 
 def _phase_align(v: np.ndarray, x0: np.ndarray) -> np.ndarray:
@@ -1175,6 +1181,42 @@ def local_expectation1(psi: CanonicalIMPS, site: int, O: np.ndarray) -> complex:
     AC = psi.AC[site]
     E = np.einsum("aub,us,asb->", AC.conj(), O, AC)
     return E / state_dot(psi, psi)
+
+
+# --------------------------------------------------------------------------
+# Energy gradients.  No counterpart in the reference: an extension for
+# gradient-based optimisation, derived from the energy functional above.  The
+# right environments solve the adjoint of the left fixed-point system, so each
+# derivative is one contraction with the converged environments.  Pinned by
+# central finite differences in the tests (no reference values exist).
+# --------------------------------------------------------------------------
+def energy_grad_mpo(psi: CanonicalIMPS, H: SchurMPO, envs: DMRGCache) -> List[np.ndarray]:
+    """``dE/dW[site][i,u,j,s] = sum conj(AC[b,u,c']) GL[b,i,a] AC[a,s,c] GR[c,j,c']``
+    for every site, with the two identity blocks of the Schur form set to zero."""
+    out = []
+    for l in range(len(psi)):
+        AC = psi.AC[l]
+        G = np.einsum("buc,bia,asd,djc->iujs", AC.conj(), envs.lefts[l], AC, envs.rights[l], optimize=True)
+        G = np.asfortranarray(G)
+        m, n = G.shape[0], G.shape[2]
+        G[0, :, 0, :] = 0.0
+        G[m - 1, :, n - 1, :] = 0.0
+        out.append(G)
+    return out
+
+
+def energy_grad_al(psi: CanonicalIMPS, H: SchurMPO, envs: DMRGCache) -> List[np.ndarray]:
+    """Wirtinger gradient ``dE/dconj(AL[site]) = (H_AC(AC) - lambda AC) C^H`` of the
+    normalised energy of the uniform MPS generated by ``AL``."""
+    out = []
+    for l in range(len(psi)):
+        AC = psi.AC[l]
+        y = ac_apply(envs.lefts[l], H[l], envs.rights[l], AC)
+        lam = np.vdot(AC, y) / np.vdot(AC, AC)
+        Dl, d, Dr = AC.shape
+        g = freshape(y - lam * AC, (Dl * d, Dr)) @ psi.C[l].conj().T
+        out.append(np.asfortranarray(freshape(g, (Dl, d, Dr))))
+    return out
 
 
 # --------------------------------------------------------------------------
