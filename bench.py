@@ -48,11 +48,15 @@ def parse():
                         "residual (the mixed-precision form); fp64: the plain FP64 pipeline")
     p.add_argument("--nslices", type=int, default=0, help="int8 slices (0 = adaptive to the solver tolerance)")
     p.add_argument("--D", type=int, default=WORKLOAD["D"])
-    p.add_argument("--mode", default="vumps", choices=["vumps", "heff", "converge", "tdvp"],
+    p.add_argument("--mode", default="vumps", choices=["vumps", "heff", "converge", "tdvp", "batch"],
                    help="vumps: one VUMPS iteration per step; heff: one AC Heff apply per step; "
                         "converge: VUMPS to convergence in FP64 and split precision from the same start; "
-                        "tdvp: TFIM quench, TDVP in FP64 and split precision from one ground state")
+                        "tdvp: TFIM quench, TDVP in FP64 and split precision from one ground state; "
+                        "batch: 64 TFIM instances of uneven D by batched VUMPS, with dE/dh checks")
     p.add_argument("--tdvp-steps", type=int, default=200)
+    p.add_argument("--instances", type=int, default=64)
+    p.add_argument("--threads", type=int, default=16)
+    p.add_argument("--no-seq", action="store_true")
     p.add_argument("--model", default="hubbard", choices=["tfim", "xxz", "hubbard"])
     p.add_argument("--N", type=int, default=None)
     p.add_argument("--h", type=float, default=1.0, help="TFIM field")
@@ -228,11 +232,14 @@ def run_ours(args, world, rank, local):
     torch.cuda.synchronize()
     e0.record(stream)
     infos = []
+    # NVTX range of the timed iterations (profilers can restrict capture to it)
+    torch.cuda.nvtx.range_push("vumps_timed")
     for _ in range(args.steps):
         it += 1
         info = step(it, eps)
         eps = info.galerkin
         infos.append(info)
+    torch.cuda.nvtx.range_pop()
     e1.record(stream)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
@@ -474,6 +481,101 @@ def run_tdvp(args, world, rank, local):
             "sample_every_steps": every}
 
 
+def run_batch(args, world, rank, local):
+    """Batched VUMPS over 64 TFIM instances (J=1, h ~ U[0.5, 1.5] and D from
+    {32, 64, 128, 256, 512}, both drawn with seed 5; instance k starts from random
+    site tensors with seed 1000 + k), split precision, each instance on its own
+    context and stream.  Reports aggregate VUMPS iterations/s and the wall time to
+    solve all of them, the same instances solved one after another on one stream,
+    energies against the exact TFIM energy, and dE/dh from the adjoint contraction
+    against Hellmann-Feynman (all instances) and central differences of converged
+    energies (the four smallest instances, FP64, dh = 1e-5)."""
+    import torch
+    import math as _m
+    from scipy.integrate import quad
+    import infinitempsalgorithms_b200 as imps
+    from infinitempsalgorithms_b200 import _lib as L
+    torch.cuda.set_device(local)
+    rng = np.random.default_rng(5)
+    n = args.instances
+    hs = rng.uniform(0.5, 1.5, n)
+    Ds = rng.choice([32, 64, 128, 256, 512], n)
+    Hs = [imps.tfim_hamiltonian(1.0, float(h)) for h in hs]
+    As = [imps.random_site_tensors([2], int(D), 1000 + k) for k, D in enumerate(Ds)]
+    alg = imps.VUMPS(maxiter=args.maxiter, tol=args.tol)
+
+    def e0(h):
+        return -quad(lambda k: _m.sqrt(1 + h * h - 2 * h * _m.cos(k)), 0, _m.pi)[0] / _m.pi
+
+    def make(ctxs):
+        return [imps.CanonicalIMPS.from_sites(As[k], ctx=ctxs[k]) for k in range(n)]
+    res = {}
+    # concurrent: one context (stream) per instance
+    ctxs = [imps.Context(local) for _ in range(n)]
+    for c in ctxs:
+        c.set_precision(L.IMPS_PREC_SPLIT_I8, args.nslices)
+    psi0s = make(ctxs)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    out = imps.find_groundstate_batch(psi0s, Hs, alg, nthreads=args.threads)
+    torch.cuda.synchronize()
+    wall_b = time.perf_counter() - t0
+    iters_b = sum(o[2].niter for o in out)
+    es = [imps.expectationvalue(o[0], Hs[k], o[1]).real for k, o in enumerate(out)]
+    dW = [[(imps.tfim_hamiltonian(1.0, float(h) + 1e-3).Ws[0] - imps.tfim_hamiltonian(1.0, float(h) - 1e-3).Ws[0])
+           / 2e-3] for h in hs]
+    grads = [imps.coupling_gradient(o[0], Hs[k], dW[k], o[1]).real for k, o in enumerate(out)]
+    hf = [-imps.expectationvalue(o[0], (1, imps.sigma("z"))).real for o in out]
+    res["batched"] = {"wall_s": wall_b, "iterations": int(iters_b), "iter_per_s": iters_b / wall_b,
+                      "converged": int(sum(o[2].converged for o in out)),
+                      "max_galerkin": float(max(o[2].itererr for o in out))}
+    for c in ctxs:
+        c.close()
+    # the same instances one after another on one stream
+    if not args.no_seq:
+        c1 = imps.Context(local)
+        c1.set_precision(L.IMPS_PREC_SPLIT_I8, args.nslices)
+        t0 = time.perf_counter()
+        its = 0
+        for k in range(n):
+            p0 = imps.CanonicalIMPS.from_sites(As[k], ctx=c1)
+            _, _, inf = imps.find_groundstate(p0, Hs[k], alg)
+            its += inf.niter
+        c1.synchronize()
+        wall_s = time.perf_counter() - t0
+        res["sequential"] = {"wall_s": wall_s, "iterations": its, "iter_per_s": its / wall_s}
+        c1.close()
+    # central differences of converged FP64 energies for the four smallest instances
+    fd = []
+    small = [int(k) for k in np.argsort(Ds, kind="stable")[:4]]
+    c2 = imps.Context(local)
+    tight = imps.VUMPS(maxiter=400, tol=1e-12)
+    for k in small:
+        p0 = imps.CanonicalIMPS.from_sites(As[k], ctx=c2)
+        g0, genv, _ = imps.find_groundstate(p0, Hs[k], tight)
+        dh = 1e-5
+        vals = []
+        for sgn in (1, -1):
+            Hk = imps.tfim_hamiltonian(1.0, float(hs[k]) + sgn * dh)
+            pk, ek, _ = imps.find_groundstate(g0, Hk, tight)
+            vals.append(imps.expectationvalue(pk, Hk, ek).real)
+        gk = imps.coupling_gradient(g0, Hs[k], dW[k], genv).real
+        fd.append({"instance": k, "D": int(Ds[k]), "h": float(hs[k]), "adjoint": gk,
+                   "central_difference": (vals[0] - vals[1]) / (2 * dh)})
+    c2.close()
+    value = res["batched"]["iter_per_s"]
+    return {"metric": f"batched VUMPS iterations/s ({n} TFIM instances, D in 32..512)", "value": value,
+            "unit": "iter/s", "higher_is_better": True, "n_gpus": world,
+            "config": {"workload": "vumps_tfim_batch", "instances": n, "h": "U[0.5,1.5] seed 5",
+                       "D": "from {32,64,128,256,512} seed 5", "tol": args.tol, "maxiter": args.maxiter,
+                       "threads": args.threads, "precision": "split", "nslices": args.nslices or "adaptive"},
+            **res,
+            "max_abs_e_minus_exact": float(max(abs(es[k] - e0(float(hs[k]))) for k in range(n))),
+            "max_abs_grad_minus_hellmann_feynman": float(max(abs(grads[k] - hf[k]) for k in range(n))),
+            "fd_check": fd,
+            "max_abs_grad_minus_fd": float(max(abs(f["adjoint"] - f["central_difference"]) for f in fd))}
+
+
 def snapshot(ctx, psi, envs):
     """Host copies of the state tensors and the environments (used to replay iterations)."""
     from infinitempsalgorithms_b200 import _lib as L
@@ -633,6 +735,11 @@ def main():
         return
     if args.mode == "converge":
         res = run_converge(args, world, rank, local)
+        if rank == 0:
+            print(json.dumps(res))
+        return
+    if args.mode == "batch":
+        res = run_batch(args, world, rank, local)
         if rank == 0:
             print(json.dumps(res))
         return

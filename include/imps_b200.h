@@ -269,6 +269,15 @@ int imps_vumps_localupdate(imps_envs* envs, const imps_mpo* mpo, imps_state* st,
 /* One full VUMPS iteration (vumps.jl:296-318) for the outer-loop index `iter`
  * (1-based) and the previous Galerkin error `eps`, with the reference's dynamic
  * tolerances (Defaults, src/utility.jl:308-320). */
+/* Batched group of imps_vumps_iter calls over n independent instances (e.g. many
+ * Hamiltonians with uneven bond dimensions).  Instances on distinct contexts run
+ * concurrently, one host thread and one stream per context (at most nthreads
+ * threads; <= 0 means 16); instances sharing a context run in order.  status[i] is
+ * each instance's own status; the return value is the most severe error, else
+ * IMPS_OK.  No counterpart in the reference, whose instances would be separate
+ * find_groundstate calls (vumps.jl:296-318). */
+int imps_vumps_iter_batch(int n, imps_envs* const* envs, const imps_mpo* const* mpos, imps_state* const* states,
+                          const int* iters, const double* eps, imps_vumps_info* infos, int* status, int nthreads);
 int imps_vumps_iter(imps_envs* envs, const imps_mpo* mpo, imps_state* st, int iter, double eps,
                     imps_vumps_info* info);
 /* timestep(psi, H, dt, TDVP(), envs) (src/algorithms/timeevo/tdvp.jl:34-53). */

@@ -128,6 +128,8 @@ _SIGS = {
     "imps_energy_grad_al": (I32, [P, P, P, I32, DP]),
     "imps_vumps_localupdate": (I32, [P, P, P, D, I32, I32, I32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "imps_vumps_iter": (I32, [P, P, P, I32, D, C.POINTER(VumpsInfo)]),
+    "imps_vumps_iter_batch": (I32, [I32, C.POINTER(P), C.POINTER(P), C.POINTER(P), C.POINTER(I32), DP,
+                                    C.POINTER(VumpsInfo), C.POINTER(I32), I32]),
     "imps_tdvp_step": (I32, [P, P, P, D, D, D, I32, I32, D, I32, C.POINTER(KrylovInfo)]),
     "imps_idmrg_sweep": (I32, [P, P, P, D, I32, I32, I32, DP, DP]),
 }

@@ -28,7 +28,7 @@ __all__ = [
     "C_hamiltonian", "fixedpoint", "integrate", "regauge", "calc_galerkin", "expectationvalue", "VUMPS",
     "IDMRG", "TDVP", "IterativeConvergenceInfo", "find_groundstate", "timestep", "time_evolve", "linsolve",
     "qrpos", "lqpos", "push_env_left", "push_env_right", "push_mpo_left", "push_mpo_right",
-    "energy_gradient_mpo", "energy_gradient_AL", "coupling_gradient", "rrule_energy",
+    "energy_gradient_mpo", "energy_gradient_AL", "coupling_gradient", "rrule_energy", "find_groundstate_batch",
 ]
 
 
@@ -901,6 +901,65 @@ def find_groundstate(psi0, H: SparseIMPO, alg=None, envs: Optional[DMRGCache] = 
             converged = True
             break
     return psi, envs, IterativeConvergenceInfo(it, converged, losses, losses[-1])
+
+
+def find_groundstate_batch(psi0s: Sequence[CanonicalIMPS], Hs: Sequence[SparseIMPO], alg: Optional[VUMPS] = None,
+                           nthreads: int = 16):
+    """VUMPS on many independent instances at once -> list of ``(psi, envs, info)``.
+
+    No counterpart in the reference (which would call ``find_groundstate`` per
+    instance).  Instances on distinct contexts advance concurrently, one host
+    thread and one CUDA stream each (``imps_vumps_iter_batch``); every instance
+    follows the default tolerance schedule of ``find_groundstate(::VUMPS)`` and
+    stops on its own Galerkin error or ``alg.maxiter``."""
+    from concurrent.futures import ThreadPoolExecutor
+    alg = alg or VUMPS()
+    n = len(psi0s)
+    psis = [p.copy() for p in psi0s]
+
+    def setup(i):
+        envs = DMRGCache(psis[i], Hs[i])
+        eps = calc_galerkin(psis[i], Hs[i], envs)
+        ae = updatetol(alg.alg_environments, 0, eps)
+        recalculate(envs, psis[i], Hs[i], tol=ae["tol"], maxiter=ae["maxiter"])
+        return envs, eps
+    # instances sharing a context share its scratch buffers: one host thread per context
+    groups = {}
+    for i in range(n):
+        groups.setdefault(id(psis[i].ctx), []).append(i)
+    res = [None] * n
+
+    def setup_group(idx):
+        for i in idx:
+            res[i] = setup(i)
+    with ThreadPoolExecutor(max_workers=max(1, min(nthreads, len(groups)))) as ex:
+        list(ex.map(setup_group, groups.values()))
+    envss = [r[0] for r in res]
+    eps = [r[1] for r in res]
+    losses = [[e] for e in eps]
+    iters = [0] * n
+    converged = [False] * n
+    active = [i for i in range(n) if alg.maxiter > 0]
+    lib = psis[0].ctx.lib if n else None
+    while active:
+        k = len(active)
+        E = (C.c_void_p * k)(*[envss[i].h for i in active])
+        M = (C.c_void_p * k)(*[Hs[i].handle(psis[i].ctx) for i in active])
+        S = (C.c_void_p * k)(*[psis[i].h for i in active])
+        it = (C.c_int * k)(*[iters[i] + 1 for i in active])
+        ep = (C.c_double * k)(*[eps[i] for i in active])
+        infos = (L.VumpsInfo * k)()
+        st = (C.c_int * k)()
+        lib.imps_vumps_iter_batch(k, E, M, S, it, ep, infos, st, nthreads)
+        for j, i in enumerate(active):
+            check(st[j], psis[i].ctx.h)
+            iters[i] += 1
+            eps[i] = infos[j].galerkin
+            losses[i].append(eps[i])
+            converged[i] = eps[i] <= alg.tol
+        active = [i for i in active if not converged[i] and iters[i] < alg.maxiter]
+    return [(psis[i], envss[i], IterativeConvergenceInfo(iters[i], converged[i], losses[i], losses[i][-1]))
+            for i in range(n)]
 
 
 def _find_groundstate_idmrg(psi0, H, alg: IDMRG, envs=None):

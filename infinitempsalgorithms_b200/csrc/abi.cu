@@ -1,8 +1,12 @@
 // The extern "C" boundary (include/imps_b200.h).  Every entry point catches
 // exceptions and maps them to IMPS_* status codes; the message is kept in the
 // context (imps_ctx_last_error) and in a thread-local fallback.
+#include <algorithm>
+#include <atomic>
 #include <cstdlib>
 #include <cstring>
+#include <thread>
+#include <vector>
 #include <string>
 
 #include "algos.h"
@@ -895,6 +899,42 @@ int imps_vumps_iter(imps_envs* E, const imps_mpo* mpo, imps_state* st, int iter,
     if (info) *info = v;
     return IMPS_OK;
   });
+}
+
+int imps_vumps_iter_batch(int n, imps_envs* const* envs, const imps_mpo* const* mpos, imps_state* const* states,
+                          const int* iters, const double* eps, imps_vumps_info* infos, int* status, int nthreads) {
+  if (n < 0 || (n > 0 && (!envs || !mpos || !states || !iters || !eps || !infos || !status))) return IMPS_INVALID_ARG;
+  if (n == 0) return IMPS_OK;
+  // instances that share a context run one after another on one host thread; distinct
+  // contexts (distinct streams) run on concurrent host threads
+  std::vector<imps::Context*> keys;
+  std::vector<std::vector<int>> groups;
+  for (int i = 0; i < n; ++i) {
+    if (!envs[i] || !mpos[i] || !states[i]) return IMPS_INVALID_ARG;
+    imps::Context* c = envs[i]->ctx;
+    auto it = std::find(keys.begin(), keys.end(), c);
+    if (it == keys.end()) {
+      keys.push_back(c);
+      groups.emplace_back();
+      groups.back().push_back(i);
+    } else {
+      groups[it - keys.begin()].push_back(i);
+    }
+  }
+  std::atomic<int> next{0};
+  auto worker = [&] {
+    for (int g = next.fetch_add(1); g < (int)groups.size(); g = next.fetch_add(1))
+      for (int i : groups[g]) status[i] = imps_vumps_iter(envs[i], mpos[i], states[i], iters[i], eps[i], &infos[i]);
+  };
+  const int nt = std::max(1, std::min<int>(nthreads > 0 ? nthreads : 16, (int)groups.size()));
+  std::vector<std::thread> pool;
+  for (int t = 1; t < nt; ++t) pool.emplace_back(worker);
+  worker();
+  for (auto& t : pool) t.join();
+  int worst = IMPS_OK;
+  for (int i = 0; i < n; ++i)
+    if (status[i] < 0 && (worst >= 0 || status[i] < worst)) worst = status[i];
+  return worst;
 }
 
 int imps_tdvp_step(imps_envs* E, const imps_mpo* mpo, imps_state* st, double dt_re, double dt_im, double tol,

@@ -13,15 +13,21 @@
 // epilogue adds r_i c_j 2^-7(d+2) acc to the FP64 output.  Truncation error per
 // element is below 2^-7s of the row/column scale.
 //
-// GEMM kernel: persistent, one CTA per SM, warp-specialised, 128 x 128 output tiles:
-//   warp 0: TMA producer (cp.async.bulk.tensor, 128B swizzle, 6-stage ring of
-//           16 KB A + 16 KB B stages)
-//   warp 1: TMEM allocator + single-thread tcgen05.mma issuer (M=128, N=128, K=32);
-//           every slice diagonal of a tile accumulates in its own int32 TMEM slot
-//           (4 slots x 128 columns)
+// GEMM kernel: persistent, one CTA per SM, warp-specialised, 128 x 64 output tiles.
+// K runs outermost: one pipeline stage holds a 64-byte K block of *every* slice
+// plane of both operands, and the MMA thread issues all slice pairs (ta, tb) with
+// ta + tb < s for it, each diagonal d = ta + tb into its own int32 TMEM
+// accumulator (s x 64 columns per tile).  Every byte brought into shared memory
+// thus feeds (s + 1) / 2 MMAs on average instead of one, which is what keeps the
+// tensor pipe fed from L2.
+//   warp 0: TMA producer (cp.async.bulk.tensor, 64B swizzle, 2-8 stages by s)
+//   warp 1: TMEM allocator + single-thread tcgen05.mma issuer (M=128, N=64, K=32)
 //   warps 2-9: epilogue, tcgen05.ld 32x32b, two warps per TMEM lane quarter; each
-//           thread keeps the FP64 partial sums of its row over all diagonals in
-//           registers and writes the tile once
+//           thread keeps the FP64 sums of its row over all diagonals in registers
+//           and writes the tile once.  With s <= 4 two tiles' accumulators fit in
+//           TMEM, so the epilogue of one tile overlaps the MMAs of the next.
+// The K extent is cut into groups so that no int32 sum can overflow: the largest
+// diagonal adds s pairs, so a group spans fewer than 2^31 / (127^2 s) bytes.
 // Every mbarrier wait is bounded (~1 s of clock64); on expiry the kernel sets an
 // error flag, drains and returns, and the host raises IMPS_TIMEOUT.
 #include <cuda.h>
@@ -40,17 +46,34 @@ namespace imps {
 namespace {
 
 constexpr int BM = 128;          // tile rows (real rows of At)
-constexpr int BN = 128;          // tile cols (rows of Bt)
-constexpr int BKB = 128;         // K bytes per stage (one 128B swizzle atom)
-constexpr int STAGES = 6;
-constexpr int NSLOT = 4;         // TMEM accumulator slots of BN columns (4 x 128 = 512)
+constexpr int BN = 64;           // tile cols (rows of Bt)
+constexpr int KB = 64;           // K bytes per pipeline stage (one 64B swizzle row)
+constexpr int KPAD = 128;        // K padding of the slice planes (the slicing kernels' tile)
+constexpr int MAX_STAGES = 8;
+constexpr int MAX_BUF = 4;       // tile accumulator buffers in TMEM
 constexpr int EPI_WARPS = 8;     // two warps per TMEM lane quarter, each owning BN/2 columns
-constexpr int A_STAGE = BM * BKB;   // 16 KB
-constexpr int B_STAGE = BN * BKB;   // 16 KB
-constexpr int SMEM_TILES = STAGES * (A_STAGE + B_STAGE);
-constexpr int SMEM_BYTES = SMEM_TILES + 1024 /*align*/ + 256 /*barriers*/;
+constexpr int A_TILE = BM * KB;  // 8 KB per slice
+constexpr int B_TILE = BN * KB;  // 4 KB per slice
+constexpr int STAGE_BUDGET = 200 * 1024;
+constexpr int BAR_BYTES = 512;
 constexpr int NTHREADS = 32 * (2 + EPI_WARPS);
 constexpr long long WAIT_CYCLES = 2000000000LL;   // ~1 s at 1.9 GHz
+
+__host__ __device__ constexpr int stages_for(int s) {
+  return (STAGE_BUDGET / (s * (A_TILE + B_TILE))) < MAX_STAGES ? (STAGE_BUDGET / (s * (A_TILE + B_TILE)))
+                                                               : MAX_STAGES;
+}
+__host__ __device__ constexpr int bufs_for(int s) {
+  return (512 / (s * BN)) < MAX_BUF ? (512 / (s * BN)) : MAX_BUF;
+}
+__host__ constexpr int smem_bytes_for(int s) { return stages_for(s) * s * (A_TILE + B_TILE) + 1024 + BAR_BYTES; }
+__host__ constexpr int max_smem_bytes() {
+  int m = 0;
+  for (int s = 1; s <= 8; ++s) m = smem_bytes_for(s) > m ? smem_bytes_for(s) : m;
+  return m;
+}
+static_assert(max_smem_bytes() <= 227 * 1024, "pipeline does not fit in shared memory");
+static_assert(stages_for(8) >= 2, "at least double buffering at 8 slices");
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -99,18 +122,18 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, u
       : "memory");
 }
 
-// UMMA shared-memory descriptor: K-major, 128B swizzle, 8-row groups 1024 B apart.
+// UMMA shared-memory descriptor: K-major, 64B swizzle, 8-row groups 512 B apart.
 __device__ __forceinline__ uint64_t make_desc(uint32_t saddr) {
   uint64_t d = 0;
   d |= (uint64_t)((saddr >> 4) & 0x3FFF);          // start address
-  d |= (uint64_t)1 << 16;                           // leading byte offset (unused for SW128 K-major)
-  d |= (uint64_t)(1024 >> 4) << 32;                 // stride byte offset
+  d |= (uint64_t)1 << 16;                           // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(512 >> 4) << 32;                  // stride byte offset: 8 rows x 64 B
   d |= (uint64_t)1 << 46;                           // descriptor version (sm100)
-  d |= (uint64_t)2 << 61;                           // SWIZZLE_128B
+  d |= (uint64_t)4 << 61;                           // SWIZZLE_64B
   return d;
 }
 
-// instruction descriptor: kind::i8, s8 x s8 -> s32, both K-major, M = 128, N = 256
+// instruction descriptor: kind::i8, s8 x s8 -> s32, both K-major, M = 128, N = 64
 __host__ __device__ constexpr uint32_t make_idesc() {
   return (2u << 4)                 // D format: s32
          | (1u << 7)               // A format: s8
@@ -147,7 +170,9 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, int32_t* r) {
 struct GemmArgs {
   int num_m, num_n;          // tiles
   int n_fast;                // raster: 1 -> consecutive tiles walk N (A is the larger operand)
-  int kblocks;               // K blocks of 128 bytes per slice plane
+  int kblocks;               // K blocks of KB bytes per slice plane
+  int nst;                   // pipeline stages (by s)
+  int nbuf;                  // tile accumulator buffers in TMEM (by s)
   int s;                     // slice diagonals d = 0 .. s-1
   double2* C;                // complex output
   int64_t ldc;
@@ -159,19 +184,16 @@ struct GemmArgs {
   int* err;
 };
 
-// Accumulation groups of one tile: diagonal d, K range [kb0, kb1) of every slice pair (ta, d - ta).
+// Accumulation groups of one tile: K range [kb0, kb1) of every slice pair; the
+// largest diagonal sums s pairs of products <= 127^2, so a group stays below 2^31.
 struct GroupIter {
   const GemmArgs* g;
-  int d = 0, kb0 = 0;
+  int kb0 = 0;
   __device__ explicit GroupIter(const GemmArgs* a) : g(a) {}
-  __device__ bool valid() const { return d < g->s; }
-  // (d+1) pairs x chunk bytes x 127^2 must stay below 2^31 in the int32 accumulator
-  __device__ static int chunk(int d) { return max(1, (int)(2147483647.0 / (16129.0 * (d + 1) * BKB))); }
-  __device__ int kb1() const { return min(g->kblocks, kb0 + chunk(d)); }
-  __device__ void next() {
-    kb0 += chunk(d);
-    if (kb0 >= g->kblocks) { kb0 = 0; ++d; }
-  }
+  __device__ bool valid() const { return kb0 < g->kblocks; }
+  __device__ int chunk() const { return max(1, (int)(2147483647.0 / (16129.0 * g->s * KB))); }
+  __device__ int kb1() const { return min(g->kblocks, kb0 + chunk()); }
+  __device__ void next() { kb0 += chunk(); }
 };
 
 __device__ __forceinline__ void tile_coords(const GemmArgs& g, int t, int& mb, int& nb) {
@@ -179,28 +201,54 @@ __device__ __forceinline__ void tile_coords(const GemmArgs& g, int t, int& mb, i
   else { mb = t % g.num_m; nb = t / g.num_m; }
 }
 
+// Issues the slice-pair MMAs of one stage: for every diagonal d and pair (ta, d - ta),
+// two K=32 MMAs into the diagonal's accumulator.  With a compile-time slice count the
+// loops unroll into a straight run of MMAs on precomputed descriptors, so one thread
+// keeps up with the tensor pipe.
+template <int SC>
+__device__ __forceinline__ void issue_stage(int S, uint64_t da, uint64_t db, uint32_t dt0, uint32_t idesc, bool fresh) {
+  const int s = SC > 0 ? SC : S;
+#pragma unroll
+  for (int d = 0; d < (SC > 0 ? SC : 8); ++d) {
+    if (d >= s) break;
+    const uint32_t dtmem = dt0 + (uint32_t)(d * BN);
+#pragma unroll
+    for (int ta = 0; ta <= d; ++ta) {
+      const int tb = d - ta;
+#pragma unroll
+      for (int kk = 0; kk < KB / 32; ++kk) {
+        // start-address field counts 16-byte units
+        const uint64_t a = da + (uint64_t)((ta * A_TILE + kk * 32) >> 4);
+        const uint64_t b = db + (uint64_t)((tb * B_TILE + kk * 32) >> 4);
+        umma_i8(dtmem, a, b, idesc, (fresh && ta == 0 && kk == 0) ? 0u : 1u);
+      }
+    }
+  }
+}
+
+template <int SC>
 __global__ void __launch_bounds__(NTHREADS, 1)
     k_gemm_i8(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, const GemmArgs g) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  uint8_t* sA = smem;
-  uint8_t* sB = smem + STAGES * A_STAGE;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + SMEM_TILES);
-  uint64_t* full = bars;                       // [STAGES]
-  uint64_t* empty = bars + STAGES;             // [STAGES]
-  uint64_t* tfull = bars + 2 * STAGES;         // [NSLOT]
-  uint64_t* tempty = bars + 2 * STAGES + NSLOT;  // [NSLOT]
-  uint64_t* drain = bars + 2 * STAGES + 2 * NSLOT;  // MMA drain on the error path
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * STAGES + 2 * NSLOT + 1);
+  const int S = SC > 0 ? SC : g.s, NST = g.nst, NBUF = g.nbuf;
+  const int stage_bytes = S * (A_TILE + B_TILE);  // [A slices][B slices]
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + NST * stage_bytes);
+  uint64_t* full = bars;                                  // [MAX_STAGES]
+  uint64_t* empty = bars + MAX_STAGES;                    // [MAX_STAGES]
+  uint64_t* tfull = bars + 2 * MAX_STAGES;                // [MAX_BUF]
+  uint64_t* tempty = bars + 2 * MAX_STAGES + MAX_BUF;     // [MAX_BUF]
+  uint64_t* drain = bars + 2 * MAX_STAGES + 2 * MAX_BUF;  // MMA drain on the error path
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * MAX_STAGES + 2 * MAX_BUF + 1);
   volatile int* err = g.err;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
-    for (int st = 0; st < STAGES; ++st) {
+    for (int st = 0; st < NST; ++st) {
       mbar_init(&full[st], 1);
       mbar_init(&empty[st], 1);
     }
-    for (int a = 0; a < NSLOT; ++a) {
+    for (int a = 0; a < NBUF; ++a) {
       mbar_init(&tfull[a], 1);
       mbar_init(&tempty[a], EPI_WARPS);  // one arrival per epilogue warp
     }
@@ -222,29 +270,26 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       int stage = 0;
       uint32_t phase = 0;
       bool ok = true;
-      int issued[STAGES];  // parity of the last load issued into each stage (-1: none)
-      for (int s2 = 0; s2 < STAGES; ++s2) issued[s2] = -1;
+      int issued[MAX_STAGES];  // parity of the last load issued into each stage (-1: none)
+      for (int s2 = 0; s2 < MAX_STAGES; ++s2) issued[s2] = -1;
       for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
         int mb, nb;
         tile_coords(g, t, mb, nb);
-        for (GroupIter gi(&g); gi.valid() && ok; gi.next()) {
-          const int kb1 = gi.kb1();
-          for (int ta = 0; ta <= gi.d && ok; ++ta) {
-            const int tb = gi.d - ta;
-            for (int kb = gi.kb0; kb < kb1; ++kb) {
-              ok = mbar_wait(&empty[stage], phase ^ 1, err);
-              if (!ok) break;
-              mbar_expect_tx(&full[stage], A_STAGE + B_STAGE);
-              tma_load_3d(sA + stage * A_STAGE, &mapA, &full[stage], kb * BKB, mb * BM, ta);
-              tma_load_3d(sB + stage * B_STAGE, &mapB, &full[stage], kb * BKB, nb * BN, tb);
-              issued[stage] = (int)phase;
-              if (++stage == STAGES) { stage = 0; phase ^= 1; }
-            }
+        for (int kb = 0; kb < g.kblocks && ok; ++kb) {
+          ok = mbar_wait(&empty[stage], phase ^ 1, err);
+          if (!ok) break;
+          uint8_t* base = smem + stage * stage_bytes;
+          mbar_expect_tx(&full[stage], (uint32_t)stage_bytes);
+          for (int sl = 0; sl < S; ++sl) {
+            tma_load_3d(base + sl * A_TILE, &mapA, &full[stage], kb * KB, mb * BM, sl);
+            tma_load_3d(base + S * A_TILE + sl * B_TILE, &mapB, &full[stage], kb * KB, nb * BN, sl);
           }
+          issued[stage] = (int)phase;
+          if (++stage == NST) { stage = 0; phase ^= 1; }
         }
       }
       // every issued copy must land before the CTA may exit (bounded)
-      for (int s2 = 0; s2 < STAGES; ++s2) {
+      for (int s2 = 0; s2 < NST; ++s2) {
         if (issued[s2] < 0) continue;
         long long t0 = clock64();
         while (!mbar_try(&full[s2], (uint32_t)issued[s2]) && clock64() - t0 < WAIT_CYCLES) {
@@ -256,34 +301,28 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       const uint32_t idesc = make_idesc();
       int stage = 0;
       uint32_t phase = 0;
-      int grp = 0;  // accumulation-group counter (selects the TMEM slot)
+      int grp = 0;  // accumulation-group counter (selects the TMEM buffer)
       bool ok = true;
       for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
         for (GroupIter gi(&g); gi.valid() && ok; gi.next(), ++grp) {
-          const int acc = grp % NSLOT;
-          ok = mbar_wait(&tempty[acc], ((grp / NSLOT) & 1) ^ 1, err);
+          const int buf = grp % NBUF;
+          ok = mbar_wait(&tempty[buf], ((grp / NBUF) & 1) ^ 1, err);
           if (!ok) break;
           tc_fence_after();
-          const uint32_t dtmem = tmem_base + acc * BN;
           const int kb1 = gi.kb1();
-          bool first = true;
-          for (int ta = 0; ta <= gi.d && ok; ++ta) {
-            for (int kb = gi.kb0; kb < kb1; ++kb) {
-              ok = mbar_wait(&full[stage], phase, err);
-              if (!ok) break;
-              tc_fence_after();
-              const uint32_t a0 = smem_u32(sA + stage * A_STAGE), b0 = smem_u32(sB + stage * B_STAGE);
-#pragma unroll
-              for (int kk = 0; kk < BKB / 32; ++kk) {
-                umma_i8(dtmem, make_desc(a0 + kk * 32), make_desc(b0 + kk * 32), idesc, first ? 0u : 1u);
-                first = false;
-              }
-              umma_commit(&empty[stage]);  // frees the smem stage when these MMAs retire
-              if (++stage == STAGES) { stage = 0; phase ^= 1; }
-            }
+          for (int kb = gi.kb0; kb < kb1 && ok; ++kb) {
+            ok = mbar_wait(&full[stage], phase, err);
+            if (!ok) break;
+            tc_fence_after();
+            const uint32_t a0 = smem_u32(smem + stage * stage_bytes);
+            const uint32_t b0 = a0 + S * A_TILE;
+            issue_stage<SC>(S, make_desc(a0), make_desc(b0), tmem_base + (uint32_t)(buf * S * BN), idesc,
+                            kb == gi.kb0);
+            umma_commit(&empty[stage]);  // frees the smem stage when these MMAs retire
+            if (++stage == NST) { stage = 0; phase ^= 1; }
           }
           if (!ok) break;
-          umma_commit(&tfull[acc]);
+          umma_commit(&tfull[buf]);
         }
       }
       // all MMAs issued by this thread retire before TMEM is released (bounded)
@@ -303,26 +342,25 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
       int mb, nb;
       tile_coords(g, t, mb, nb);
-      // FP64 partial sums of this thread's row over all slice diagonals of the tile
+      // FP64 sums of this thread's row over all slice diagonals and K groups of the tile
       double part[HC];
 #pragma unroll
       for (int j = 0; j < HC; ++j) part[j] = 0.0;
       bool ok = true;
       for (GroupIter gi(&g); gi.valid(); gi.next(), ++grp) {
-        const int acc = grp % NSLOT;
-        if (!mbar_wait(&tfull[acc], (grp / NSLOT) & 1, err)) { ok = false; break; }
+        const int buf = grp % NBUF;
+        if (!mbar_wait(&tfull[buf], (grp / NBUF) & 1, err)) { ok = false; break; }
         tc_fence_after();
-        const double w = ldexp(1.0, -7 * (gi.d + 2));
-#pragma unroll
-        for (int cc = 0; cc < HC / 32; ++cc) {
+        for (int d = 0; d < S; ++d) {
+          const double w = ldexp(1.0, -7 * (d + 2));
           int32_t r[32];
-          tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + acc * BN + h * HC + cc * 32, r);
+          tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)((buf * S + d) * BN + h * HC), r);
 #pragma unroll
-          for (int j = 0; j < 32; ++j) part[cc * 32 + j] = fma((double)r[j], w, part[cc * 32 + j]);
+          for (int j = 0; j < 32; ++j) part[j] = fma((double)r[j], w, part[j]);
         }
         tc_fence_before();
         __syncwarp();
-        if (lane == 0) mbar_arrive(&tempty[acc]);
+        if (lane == 0) mbar_arrive(&tempty[buf]);
       }
       if (!ok) break;
       const int rr = mb * BM + row;           // real row of At
@@ -544,16 +582,16 @@ PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
   return fn;
 }
 
-// 3D map over int8 planes: dims (Kp bytes, rows, planes), box (128, box_rows, 1), 128B swizzle
+// 3D map over int8 planes: dims (Kp bytes, rows, planes), box (KB, box_rows, 1), 64B swizzle
 CUtensorMap make_map(const int8_t* base, int64_t Kp, int64_t rows, int planes, int box_rows) {
   CUtensorMap m;
   std::memset(&m, 0, sizeof(m));
   cuuint64_t dims[3] = {(cuuint64_t)Kp, (cuuint64_t)rows, (cuuint64_t)planes};
   cuuint64_t strides[2] = {(cuuint64_t)Kp, (cuuint64_t)(Kp * rows)};
-  cuuint32_t box[3] = {(cuuint32_t)BKB, (cuuint32_t)box_rows, 1};
+  cuuint32_t box[3] = {(cuuint32_t)KB, (cuuint32_t)box_rows, 1};
   cuuint32_t estr[3] = {1, 1, 1};
   CUresult r = get_encode()(&m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<int8_t*>(base), dims, strides, box, estr,
-                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   IMPS_REQUIRE(r == CUDA_SUCCESS, IMPS_CUDA_ERROR, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
   return m;
@@ -571,7 +609,7 @@ void split_operand_a(Context* ctx, SplitOperand& S, Op op, int M, int K, const d
   S.K = K;
   S.s = s;
   S.Rp = round_up(2 * (int64_t)M, BM);
-  S.Kp = round_up(2 * (int64_t)K, BKB);
+  S.Kp = round_up(2 * (int64_t)K, KPAD);
   const size_t plane = (size_t)S.Rp * S.Kp;
   S.data.ensure(plane * s);
   S.scale.ensure((size_t)M * sizeof(double));
@@ -605,7 +643,7 @@ void split_operand_b(Context* ctx, SplitOperand& S, Op op, int K, int N, const d
   S.K = K;
   S.s = s;
   S.Rp = round_up(N, BN);
-  S.Kp = round_up(2 * (int64_t)K, BKB);
+  S.Kp = round_up(2 * (int64_t)K, KPAD);
   const size_t plane = (size_t)S.Rp * S.Kp;
   S.data.ensure(plane * s);
   S.scale.ensure((size_t)N * sizeof(double));
@@ -639,7 +677,8 @@ void split_gemm(Context* ctx, const SplitOperand& A, const SplitOperand& B, int 
   static std::atomic<uint64_t> attr_devices{0};
   const uint64_t bit = 1ull << (ctx->device & 63);
   if (!(attr_devices.load() & bit)) {
-    IMPS_CUDA(cudaFuncSetAttribute(k_gemm_i8, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+    for (auto k : {k_gemm_i8<0>, k_gemm_i8<2>, k_gemm_i8<3>, k_gemm_i8<4>, k_gemm_i8<5>, k_gemm_i8<6>})
+      IMPS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem_bytes()));
     attr_devices.fetch_or(bit);
   }
   const CUtensorMap mapA = make_map(static_cast<const int8_t*>(A.data.ptr), A.Kp, A.Rp, A.s, BM);
@@ -651,8 +690,10 @@ void split_gemm(Context* ctx, const SplitOperand& A, const SplitOperand& B, int 
   g.num_n = (int)(B.Rp / BN);
   // stream the larger operand once: consecutive CTAs share its tile and walk the other
   g.n_fast = (A.Rp * A.s >= B.Rp * B.s) ? 1 : 0;
-  g.kblocks = (int)(A.Kp / BKB);
+  g.kblocks = (int)(A.Kp / KB);
   g.s = s;
+  g.nst = stages_for(s);
+  g.nbuf = bufs_for(s);
   g.C = C;
   g.ldc = ldc;
   g.Mc = A.rows;
@@ -667,7 +708,14 @@ void split_gemm(Context* ctx, const SplitOperand& A, const SplitOperand& B, int 
   {
     ScopedTimer tm(ctx, "gemm_split",
                    2.0 * (double)A.Rp * (double)B.Rp * (double)A.Kp * (double)(s * (s + 1) / 2));
-    k_gemm_i8<<<grid, NTHREADS, SMEM_BYTES, ctx->stream>>>(mapA, mapB, g);
+    switch (s) {
+      case 2: k_gemm_i8<2><<<grid, NTHREADS, smem_bytes_for(s), ctx->stream>>>(mapA, mapB, g); break;
+      case 3: k_gemm_i8<3><<<grid, NTHREADS, smem_bytes_for(s), ctx->stream>>>(mapA, mapB, g); break;
+      case 4: k_gemm_i8<4><<<grid, NTHREADS, smem_bytes_for(s), ctx->stream>>>(mapA, mapB, g); break;
+      case 5: k_gemm_i8<5><<<grid, NTHREADS, smem_bytes_for(s), ctx->stream>>>(mapA, mapB, g); break;
+      case 6: k_gemm_i8<6><<<grid, NTHREADS, smem_bytes_for(s), ctx->stream>>>(mapA, mapB, g); break;
+      default: k_gemm_i8<0><<<grid, NTHREADS, smem_bytes_for(s), ctx->stream>>>(mapA, mapB, g); break;
+    }
     ctx->n_kernels++;
     ctx->n_gemm++;
     IMPS_CUDA(cudaPeekAtLastError());

@@ -159,8 +159,8 @@ __global__ void __launch_bounds__(dm::NT, 1)
                  const double2* __restrict__ B, int64_t ldb, int64_t sB, double2 beta, double2* __restrict__ C,
                  int64_t ldc, int64_t sC) {
   extern __shared__ __align__(16) double2 smem_dm[];
-  double2* As = smem_dm;                      // [dm::STAGES][dm::BK][dm::LDA]
-  double2* Bs = smem_dm + dm::STAGES * dm::A_ELEMS;   // [dm::STAGES][dm::BK][dm::LDB]
+  double2* As = smem_dm;                              // [STAGES][BK][LDA]
+  double2* Bs = smem_dm + dm::STAGES * dm::A_ELEMS;   // [STAGES][BK][LDB]
   const int bz = blockIdx.z;
   A += sA * bz;
   B += sB * bz;
@@ -171,22 +171,23 @@ __global__ void __launch_bounds__(dm::NT, 1)
   const uint32_t sbase = static_cast<uint32_t>(__cvta_generic_to_shared(smem_dm));
 
   auto issue = [&](int stage, int k0) {
-    // A tile: dm::BM x dm::BK complex, 4 per thread
+    // A tile: BM x BK complex, 8 per thread
+    static_assert(dm::BM == 128 && dm::BN == 64 && dm::BK == 16 && dm::NT == 256, "load mapping assumes this tile");
 #pragma unroll
-    for (int r = 0; r < 4; ++r) {
+    for (int r = 0; r < 8; ++r) {
       int m, k;
       if (OPA == OP_N) { m = tid & 127; k = (tid >> 7) + 2 * r; }
-      else { k = tid & 7; m = (tid >> 3) + 32 * r; }
+      else { k = tid & 15; m = (tid >> 4) + 16 * r; }
       const int gm = m0 + m, gk = k0 + k;
       const bool ok = gm < M && gk < K;
       const double2* src = ok ? ((OPA == OP_N) ? A + gm + lda * (int64_t)gk : A + gk + lda * (int64_t)gm) : A;
       cp_async16(sbase + 16u * (stage * dm::A_ELEMS + k * dm::LDA + m), src, ok ? 16 : 0);
     }
-    // B tile: dm::BK x dm::BN complex, 2 per thread
+    // B tile: BK x BN complex, 4 per thread
 #pragma unroll
-    for (int r = 0; r < 2; ++r) {
+    for (int r = 0; r < 4; ++r) {
       int n, k;
-      if (OPB == OP_N) { k = tid & 7; n = (tid >> 3) + 32 * r; }
+      if (OPB == OP_N) { k = tid & 15; n = (tid >> 4) + 16 * r; }
       else { n = tid & 63; k = (tid >> 6) + 4 * r; }
       const int gn = n0 + n, gk = k0 + k;
       const bool ok = gn < N && gk < K;

@@ -51,7 +51,7 @@ def split_ctx():
     c.close()
 
 
-@pytest.mark.parametrize("M,N,K", [(64, 256, 64), (300, 520, 130), (128, 1000, 257)])
+@pytest.mark.parametrize("M,N,K", [(512, 256, 300), (300, 520, 260), (128, 1000, 300)])
 @pytest.mark.parametrize("opA,opB", [("N", "N"), ("C", "N"), ("N", "C"), ("C", "C")])
 def test_split_gemm_bit_exact_integers(split_ctx, M, N, K, opA, opB):
     rng = np.random.default_rng(M + N + K)
@@ -63,10 +63,31 @@ def test_split_gemm_bit_exact_integers(split_ctx, M, N, K, opA, opB):
     assert np.array_equal(got, ref), f"max diff {np.abs(got - ref).max()}"
 
 
+@pytest.mark.parametrize("s", [3, 4, 5, 6])
+@pytest.mark.parametrize("M,N,K", [(256, 384, 400), (64, 64, 12000)])
+def test_split_gemm_bit_exact_slice_counts(s, M, N, K):
+    # slice counts with 2 and 1 TMEM tile buffers and 5 to 2 pipeline stages, and a K
+    # long enough to be cut into several int32-safe groups at 6 slices (sizes above the
+    # split dispatch threshold M N K >= 2^25)
+    c = imps.Context(0)
+    try:
+        c.set_precision(L.IMPS_PREC_SPLIT_I8, s)
+        rng = np.random.default_rng(s * 1000 + K)
+        A = rng.integers(-100, 101, (M, K)) + 1j * rng.integers(-100, 101, (M, K))
+        B = rng.integers(-100, 101, (K, N)) + 1j * rng.integers(-100, 101, (K, N))
+        Am, Bm = dev(A), dev(B)
+        Cd = dev(np.zeros((M, N), complex))
+        L.check(c.lib.imps_zgemm(c.h, 0, 0, M, N, K, 1.0, 0.0, C.c_void_p(Am.data_ptr()), M, C.c_void_p(Bm.data_ptr()),
+                                 K, 0.0, 0.0, C.c_void_p(Cd.data_ptr()), M), c.h)
+        assert np.array_equal(host(Cd, (M, N)), A @ B)
+    finally:
+        c.close()
+
+
 def test_split_gemm_accumulate(split_ctx):
     rng = np.random.default_rng(7)
-    A = rng.integers(-50, 51, (200, 90)) + 1j * rng.integers(-50, 51, (200, 90))
-    B = rng.integers(-50, 51, (90, 300)) + 1j * rng.integers(-50, 51, (90, 300))
+    A = rng.integers(-50, 51, (200, 600)) + 1j * rng.integers(-50, 51, (200, 600))
+    B = rng.integers(-50, 51, (600, 300)) + 1j * rng.integers(-50, 51, (600, 300))
     C0 = rng.integers(-9, 10, (200, 300)).astype(complex)
     got, ref = run_gemm(split_ctx, "N", "N", A, B, Cinit=C0, beta=1.0)
     assert np.array_equal(got, ref + C0)
