@@ -131,9 +131,17 @@ KrylovResult eigsolve_c(Context* ctx, imps_envs* E, int site, const dcplx* x0, d
   return mixed_eigsolve(ctx, n, op, x0, x, tol, kdim, maxiter, eager, E->hest_c[site]);
 }
 
+// The Lanczos exponentiate has no residual refinement: its error estimate
+// (beta h_{m+1,m} |e_m^T exp(tau H_m) e_1|) assumes matvecs exact well below the
+// tolerance, which a sliced product does not give, and with inexact matvecs the
+// sub-step halving can shrink tau without end (a D=512 TFIM step did not finish
+// in 230 s in split precision; 0.44 s in FP64).  TDVP integrates in FP64 in both
+// precision modes; the environment solves of the step may still use the split
+// engine, since their GMRES refines against an FP64 residual.
 KrylovResult expo_ac(Context* ctx, imps_envs* E, const imps_mpo* H, int site, cplx dt, const dcplx* x0, dcplx* x,
                      double tol, int kdim, int maxiter) {
   const int64_t n = (int64_t)E->Dl[site] * H->sites[site % H->N].d * E->Dr[site];
+  Fp64Scope fp64(ctx);
   ConstScope cs(ctx, {E->lefts[site].ptr, E->rights[site].ptr});
   const double scale = (E->hest_ac[site] > 0 ? E->hest_ac[site] : 1.0) * std::max(std::abs(dt), 1e-300);
   TolScope ts(ctx, tol / (8.0 * scale));
@@ -143,6 +151,7 @@ KrylovResult expo_ac(Context* ctx, imps_envs* E, const imps_mpo* H, int site, cp
 
 KrylovResult expo_c(Context* ctx, imps_envs* E, int site, cplx dt, const dcplx* x0, dcplx* x, double tol, int kdim,
                     int maxiter) {
+  Fp64Scope fp64(ctx);  // see expo_ac
   const int64_t n = (int64_t)E->Dr[site] * E->Dr[site];
   const int l1 = (site + 1) % E->N;
   ensure_GLp(ctx, E, l1);
@@ -222,6 +231,7 @@ KrylovResult tdvp_step(Context* ctx, imps_envs* E, const imps_mpo* H, imps_state
     oc += st->bond_elems(l);
   }
   for (int l = 0; l < N; ++l) {
+    ProfTag tag(ctx, "expo");
     KrylovResult r1 = expo_ac(ctx, E, H, l, dt, st->AC[l].z(), pac[l], tol, kdim, maxiter);
     KrylovResult r2 = expo_c(ctx, E, l, dt, st->C[l].z(), pc[l], tol, kdim, maxiter);
     agg.numops += r1.numops + r2.numops;
@@ -229,12 +239,21 @@ KrylovResult tdvp_step(Context* ctx, imps_envs* E, const imps_mpo* H, imps_state
     agg.converged &= r1.converged & r2.converged;
     agg.normres = std::max({agg.normres, r1.normres, r2.normres});
   }
-  for (int l = 0; l < N; ++l) regauge(ctx, st->Dl(l), st->d[l], st->Dr(l), pac[l], pc[l], st->AL[l].z());
+  {
+    ProfTag tag(ctx, "regauge");
+    for (int l = 0; l < N; ++l) regauge(ctx, st->Dl(l), st->d[l], st->Dr(l), pac[l], pc[l], st->AL[l].z());
+  }
   const int DN = st->Dr(N - 1);
   DevBuf& c0 = ctx->buf("vumps_c0", (size_t)DN * DN * sizeof(dcplx));
   zcopy(ctx, (int64_t)DN * DN, st->C[N - 1].z(), c0.z());
-  from_al(ctx, st, c0.z(), gauge_tol, gauge_maxiter);
-  envs_build(ctx, E, st, H, 1e-10, 300, 30, true);
+  {
+    ProfTag tag(ctx, "gauge");
+    from_al(ctx, st, c0.z(), gauge_tol, gauge_maxiter);
+  }
+  {
+    ProfTag tag(ctx, "envs");
+    envs_build(ctx, E, st, H, 1e-10, 300, 30, true);
+  }
   return agg;
 }
 
