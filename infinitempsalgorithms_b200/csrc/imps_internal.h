@@ -303,10 +303,6 @@ void zfill(Context* ctx, int64_t n, cplx v, dcplx* x);
 void zset_identity(Context* ctx, int D, dcplx* X, int64_t ld, cplx diag);
 double dznrm2(Context* ctx, int64_t n, const dcplx* x);
 cplx zdotc(Context* ctx, int64_t n, const dcplx* x, const dcplx* y);  // sum conj(x) y
-// h[j] = sum_k conj(V[k + ldv j]) w[k], j < nv  (one fused pass over V)
-void zdotc_multi(Context* ctx, int64_t n, int nv, const dcplx* V, int64_t ldv, const dcplx* w, cplx* h_host);
-// same, and returns ||w|| from the same pass over w
-double zdotc_multi_norm(Context* ctx, int64_t n, int nv, const dcplx* V, int64_t ldv, const dcplx* w, cplx* h_host);
 // One classical Gram-Schmidt projection w <- w - V h with h = V^H w, all on the device
 // and one host synchronisation: returns ||w_new||^2, writes h (host) and, if nw_old2
 // is given, ||w_old||^2.
@@ -324,7 +320,6 @@ void zadd_diag(Context* ctx, int D, dcplx* X, int64_t ld, cplx v);
 void zfill2d(Context* ctx, int rows, int cols, cplx v, dcplx* Y, int64_t ldy);
 // X[:, lvl-slice] strided copy helpers
 void zcopy2d(Context* ctx, int rows, int cols, const dcplx* X, int64_t ldx, dcplx* Y, int64_t ldy);
-void zadd2d(Context* ctx, int rows, int cols, const dcplx* X, int64_t ldx, dcplx* Y, int64_t ldy);
 
 // Orthogonal factorizations with a non-negative real diagonal (QRpos / LQpos).
 // Q overwrites nothing: results go to Q (m x k) and R (k x n), k = min(m, n).

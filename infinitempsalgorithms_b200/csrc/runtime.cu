@@ -77,38 +77,6 @@ __global__ void k_final_sum(int nb, int ncol, const double* __restrict__ part, i
   }
 }
 
-// h[j] partials for a chunk of up to 8 basis vectors.
-template <int CH>
-__global__ void k_dotc_multi_partial(int64_t n, int nv, const dcplx* __restrict__ V, int64_t ldv,
-                                     const dcplx* __restrict__ w, double* __restrict__ part, int64_t ldp) {
-  __shared__ double sh[kRedThreads / 32];
-  double ar[CH], ai[CH];
-#pragma unroll
-  for (int j = 0; j < CH; ++j) { ar[j] = 0.0; ai[j] = 0.0; }
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    dcplx wi = w[i];
-#pragma unroll
-    for (int j = 0; j < CH; ++j) {
-      if (j < nv) {
-        dcplx p = cmulc(V[i + ldv * j], wi);
-        ar[j] += p.x;
-        ai[j] += p.y;
-      }
-    }
-  }
-#pragma unroll
-  for (int j = 0; j < CH; ++j) {
-    if (j < nv) {
-      double r = block_sum<kRedThreads>(ar[j], sh);
-      double q = block_sum<kRedThreads>(ai[j], sh);
-      if (threadIdx.x == 0) {
-        part[blockIdx.x + ldp * (2 * j)] = r;
-        part[blockIdx.x + ldp * (2 * j + 1)] = q;
-      }
-    }
-  }
-}
-
 // One block per column: out[c] = sum_i part[i + ld c] (same order as k_final_sum).
 __global__ void k_final_sum_cols(int nb, const double* __restrict__ part, int64_t ld, double* __restrict__ out) {
   __shared__ double sh[kRedThreads / 32];
@@ -435,36 +403,6 @@ cplx zdotc(Context* ctx, int64_t n, const dcplx* x, const dcplx* y) {
   return cplx(h[0], h[1]);
 }
 
-double zdotc_multi_norm(Context* ctx, int64_t n, int nv, const dcplx* V, int64_t ldv, const dcplx* w, cplx* h_host) {
-  // chunks of 8 basis vectors per pass (high occupancy beats re-reading w), then ||w||
-  if (nv > 0) zdotc_multi(ctx, n, nv, V, ldv, w, h_host);
-  return dznrm2(ctx, n, w);
-}
-
-void zdotc_multi(Context* ctx, int64_t n, int nv, const dcplx* V, int64_t ldv, const dcplx* w, cplx* h_host) {
-  if (nv <= 0) return;
-  int nb = std::min(red_blocks(n), 592);
-  constexpr int CH = 8;
-  int nchunks = (nv + CH - 1) / CH;
-  DevBuf& red = ctx->buf("red_multi", (size_t)nb * 2 * CH * nchunks * sizeof(double));
-  DevBuf& out = ctx->buf("red_multi_out", (size_t)2 * CH * nchunks * sizeof(double));
-  ScopedTimer t(ctx, "orth", (double)n * 16 * (nv + 1));
-  for (int c = 0; c < nchunks; ++c) {
-    int nvc = std::min(CH, nv - c * CH);
-    k_dotc_multi_partial<CH><<<nb, kRedThreads, 0, ctx->stream>>>(n, nvc, V + ldv * (int64_t)(c * CH), ldv, w,
-                                                                  red.d() + (size_t)nb * 2 * CH * c, nb);
-    check_launch(ctx);
-  }
-  k_final_sum<<<1, kRedThreads, 0, ctx->stream>>>(nb, 2 * CH * nchunks, red.d(), nb, out.d());
-  check_launch(ctx);
-  std::vector<double> hv(2 * CH * nchunks);
-  download(ctx, hv.data(), out.d(), hv.size() * sizeof(double));
-  for (int j = 0; j < nv; ++j) {
-    int c = j / CH, jj = j % CH;
-    h_host[j] = cplx(hv[2 * CH * c + 2 * jj], hv[2 * CH * c + 2 * jj + 1]);
-  }
-}
-
 static void gemv_common(Context* ctx, int64_t n, int nv, const dcplx* V, int64_t ldv, const cplx* coef, dcplx* w,
                         int set) {
   ScopedTimer t(ctx, "orth", (double)n * 16 * (nv + 2));
@@ -558,11 +496,6 @@ cplx ztrace_prod(Context* ctx, int D, const dcplx* L, int64_t ldl, const dcplx* 
 void zcopy2d(Context* ctx, int rows, int cols, const dcplx* X, int64_t ldx, dcplx* Y, int64_t ldy) {
   if (rows <= 0 || cols <= 0) return;
   k_copy2d<<<grid_for((int64_t)rows * cols), 256, 0, ctx->stream>>>(rows, cols, X, ldx, Y, ldy, 0);
-  check_launch(ctx);
-}
-void zadd2d(Context* ctx, int rows, int cols, const dcplx* X, int64_t ldx, dcplx* Y, int64_t ldy) {
-  if (rows <= 0 || cols <= 0) return;
-  k_copy2d<<<grid_for((int64_t)rows * cols), 256, 0, ctx->stream>>>(rows, cols, X, ldx, Y, ldy, 1);
   check_launch(ctx);
 }
 
