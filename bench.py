@@ -702,7 +702,7 @@ def iter_counts(c0, c1, steps, D, d=4, w=6):
 # default precision), taken from the library's counters in a B200 run of this
 # script (the ``op_counts_per_iter`` key of its JSON line).  The reference arm runs
 # before the GPU arm and without a GPU, so it uses these recorded counts.
-REF_COUNTS = {"ac": 74.0, "c": 66.0, "qr": 30.0, "qr_flops": 4.0e12, "other_gemm_flops": 2.0e13}
+REF_COUNTS = {"ac": 142.7, "c": 125.3, "qr": 33.0, "qr_flops": 3.642e+12, "other_gemm_flops": 2.108e+13}
 
 
 def run_reference(args, world, rank):
