@@ -1,4 +1,4 @@
-"""Non-uniform bond dimensions in the oracle (CPU only), after the reference's
+"""Non-uniform bond dimensions and physical dimensions in the oracle (CPU only), after the reference's
 test/algorithms/envs.jl:30-73: environments and energies on a unit cell with
 bond profile [2, 4, 2], and invariance of the energy under zero-padding of one
 bond (same physical state, extra Schmidt directions of weight zero)."""
@@ -83,3 +83,38 @@ def test_zero_padding_leaves_energy_unchanged():
         assert np.allclose(B @ B.conj().T, np.eye(dl), atol=1e-12)
     Ep = O.expectationvalue(psp, H, O.build_envs(psp, H)).real
     assert abs(Ep - E0) < 1e-10
+
+
+def test_heterogeneous_physical_dims():
+    # test/algorithms/envs.jl:75-126: unit cell with d = [2, 3, 2]
+    dims = [2, 3, 2]
+    psi = O.randomimps(dims, D=4, seed=3)
+    assert abs(abs(O.state_dot(psi, psi)) - 1) < 1e-10
+    for l, d in enumerate(dims):
+        assert abs(O.local_expectation1(psi, l, np.eye(d)).real - 1) < 1e-10
+    rng = np.random.default_rng(3)
+    hd = []
+    for d in dims:
+        h = rng.standard_normal((d, d)) + 1j * rng.standard_normal((d, d))
+        hd.append((h + h.conj().T) / 2)
+    H = O.SchurMPO([O.mpohamiltonian(h, []) for h in hd])
+    e0 = O.expectationvalue(psi, H, O.build_envs(psi, H)).real
+    assert np.isfinite(e0)
+    # adding lambda_l * I on every site shifts the energy per unit cell by sum(lambda)
+    Hs = O.SchurMPO([O.mpohamiltonian(h + np.eye(h.shape[0]), []) for h in hd])
+    e1 = O.expectationvalue(psi, Hs, O.build_envs(psi, Hs)).real
+    assert abs(e1 - e0 - 3.0) < 1e-10
+
+
+def test_heterogeneous_product_ground_state():
+    # diagonal on-site fields: the ground state is a product state, E = sum of minima
+    lams = [np.array([-2.0, 1.0]), np.array([-3.0, 0.0, 2.0]), np.array([-2.0, 1.0])]
+    H = O.SchurMPO([O.mpohamiltonian(np.diag(l).astype(complex), []) for l in lams])
+    ALs = []
+    for l in lams:
+        A = O.fzeros((1, len(l), 1))
+        A[0, int(np.argmin(l)), 0] = 1.0
+        ALs.append(A)
+    psi0 = O.canonical_from_AL(ALs, np.eye(1, dtype=complex))
+    psi, envs, info = O.find_groundstate(psi0, H, O.VUMPS(D=1, maxiter=200, tol=1e-10))
+    assert abs(O.expectationvalue(psi, H, envs).real - (-7.0)) < 1e-10
