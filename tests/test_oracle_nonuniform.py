@@ -1,7 +1,8 @@
-"""Non-uniform bond dimensions and physical dimensions in the oracle (CPU only), after the reference's
-test/algorithms/envs.jl:30-73: environments and energies on a unit cell with
-bond profile [2, 4, 2], and invariance of the energy under zero-padding of one
-bond (same physical state, extra Schmidt directions of weight zero)."""
+"""Non-uniform bond and physical dimensions in the oracle (CPU only), after the
+reference's test/algorithms/envs.jl:30-126: environments and energies on a unit
+cell with bond profile [2, 4, 2], invariance of the energy under zero-padding
+of one bond (same physical state, extra Schmidt directions of weight zero), and
+a unit cell with physical dimensions [2, 3, 2]."""
 import numpy as np
 
 import oracle as O
