@@ -98,6 +98,38 @@ def test_canonical_relations_and_dot():
     assert abs(O.state_dot(psi, psi) - 1) < 1e-10
 
 
+def test_dot_between_states_and_product_state():
+    # test/algorithms/api.jl:130-141 and test/states/mps.jl:1-44
+    a = O.randomimps([2, 2], D=6, seed=11)
+    b = O.randomimps([2, 2], D=6, seed=12)
+    ab, ba = O.state_dot(a, b), O.state_dot(b, a)
+    assert abs(ab) <= 1 + 1e-8
+    assert abs(ab - np.conj(ba)) < 1e-8
+    # product state |up, down>: norm 1 and <sigma_z> = +1 / -1
+    ALs = []
+    for k in (0, 1):
+        A = O.fzeros((1, 2, 1))
+        A[0, k, 0] = 1.0
+        ALs.append(A)
+    p = O.canonical_from_AL(ALs, np.eye(1, dtype=complex))
+    assert abs(O.state_dot(p, p) - 1) < 1e-12
+    assert abs(O.local_expectation1(p, 0, O.sigma("z")) - 1) < 1e-12
+    assert abs(O.local_expectation1(p, 1, O.sigma("z")) + 1) < 1e-12
+
+
+def test_gauge_fixes_from_random_tensors():
+    # test/algorithms/api.jl:150-160: left, right and mixed gauge fixes of random tensors
+    rng = np.random.default_rng(5)
+    As = [np.asfortranarray(rng.standard_normal((6, 2, 6)) + 1j * rng.standard_normal((6, 2, 6))) for _ in range(2)]
+    psi = O.canonical_from_sites(As)
+    for l in range(2):
+        A2 = O.freshape(psi.AL[l], (12, 6))
+        assert np.linalg.norm(A2.conj().T @ A2 - np.eye(6)) < 1e-10
+        B = O.freshape(psi.AR[l], (6, 12))
+        assert np.linalg.norm(B @ B.conj().T - np.eye(6)) < 1e-10
+    assert abs(np.linalg.norm(psi.AC[0]) - 1) < 1e-10
+
+
 def test_qrpos_lqpos_positive():
     rng = np.random.default_rng(3)
     M = rng.standard_normal((12, 5)) + 1j * rng.standard_normal((12, 5))
