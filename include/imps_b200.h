@@ -145,7 +145,7 @@ int imps_state_canonicalize(imps_state* st, const double* const* As, double tol,
 /* CanonicalIMPS(ALs, C0): gaugefix!(:R), AC = AL*C (src/states/canonicalmps.jl:180-195). */
 int imps_state_from_al(imps_state* st, const double* const* ALs, const double* C0, double tol, int maxiter,
                        imps_gauge_info* info);
-/* gauge_step! (src/algorithms/groundstates/vumps.jl:257-266): keep st->AL, right gauge
+/* gauge_step! (src/algorithms/groundstates/vumps.jl:23-31): keep st->AL, right gauge
  * fix from C0 = st->C[N] for AR and C, then AC = AL*C. */
 int imps_gauge_step(imps_state* st, double tol, int maxiter, imps_gauge_info* info);
 /* dot(psi, psi) (src/states/canonicalmps.jl:262-269). */
@@ -176,8 +176,12 @@ int imps_ac_apply_dev(imps_envs* envs, const imps_mpo* mpo, int site, const void
  * (Dl, d, Dr) are caller-owned device buffers, W_host the (m, d, n, d) MPO tensor
  * in host memory (<= 64 KiB).  Sizes needing more than the array
  * (16*Dl*d*Dr*(m+n) bytes) return IMPS_INVALID_ARG.  All calls share the array:
- * calls whose GPU work overlaps race.  The first call on a device looks up the
- * array's address; make it before any stream capture. */
+ * calls whose GPU work overlaps race.  The array is created (and its address
+ * looked up) by imps_ctx_create on the context's device, so create the context
+ * before the caller's allocator reserves the device memory.  The call is
+ * asynchronous: the work is queued on the context's stream and the call returns
+ * before it finishes; order GL, GR, x and y against that stream (or pass the
+ * caller's stream to imps_ctx_set_stream).  W_host is copied during the call. */
 int imps_ac_apply_noalloc(imps_ctx* ctx, int Dl, int d, int Dr, int m, int n, const double* W_host,
                           const void* GL_dev, const void* GR_dev, const void* x_dev, void* y_dev);
 /* MPO_C_Hamiltonian action (effective.jl:52-54, 72-76): GL = lefts[site+1], GR = rights[site]. */
@@ -262,11 +266,11 @@ int imps_energy_grad_mpo(imps_envs* envs, const imps_mpo* mpo, imps_state* st, i
 int imps_energy_grad_al(imps_envs* envs, const imps_mpo* mpo, imps_state* st, int site, double* g);
 
 /* -------------------------------------------------------------- algorithms */
-/* localupdate_step! (vumps.jl:241-253): per site AC and C eigensolves + regauge!,
+/* localupdate_step! (vumps.jl:7-19): per site AC and C eigensolves + regauge!,
  * candidate ALs written into st->AL. */
 int imps_vumps_localupdate(imps_envs* envs, const imps_mpo* mpo, imps_state* st, double tol, int krylovdim,
                            int maxiter, int eager, int32_t* ac_matvecs, int32_t* c_matvecs);
-/* One full VUMPS iteration (vumps.jl:296-318) for the outer-loop index `iter`
+/* One full VUMPS iteration (vumps.jl:51-85) for the outer-loop index `iter`
  * (1-based) and the previous Galerkin error `eps`, with the reference's dynamic
  * tolerances (Defaults, src/utility.jl:308-320). */
 /* Batched group of imps_vumps_iter calls over n independent instances (e.g. many
@@ -275,7 +279,7 @@ int imps_vumps_localupdate(imps_envs* envs, const imps_mpo* mpo, imps_state* st,
  * threads; <= 0 means 16); instances sharing a context run in order.  status[i] is
  * each instance's own status; the return value is the most severe error, else
  * IMPS_OK.  No counterpart in the reference, whose instances would be separate
- * find_groundstate calls (vumps.jl:296-318). */
+ * find_groundstate calls (vumps.jl:51-85). */
 int imps_vumps_iter_batch(int n, imps_envs* const* envs, const imps_mpo* const* mpos, imps_state* const* states,
                           const int* iters, const double* eps, imps_vumps_info* infos, int* status, int nthreads);
 int imps_vumps_iter(imps_envs* envs, const imps_mpo* mpo, imps_state* st, int iter, double eps,

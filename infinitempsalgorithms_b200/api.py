@@ -719,7 +719,7 @@ def push_mpo_right(R, H: SparseIMPO, site: int, A, ctx: Optional[Context] = None
 # Observables
 # ---------------------------------------------------------------------------
 def calc_galerkin(psi: CanonicalIMPS, H: SparseIMPO, envs: DMRGCache) -> float:
-    """``calc_galerkin`` (``vumps.jl:345-358``)."""
+    """``calc_galerkin`` (``vumps.jl:111-124``)."""
     e = C.c_double()
     check(psi.ctx.lib.imps_galerkin(envs.h, H.handle(psi.ctx), psi.h, C.byref(e)), psi.ctx.h)
     return e.value
@@ -861,7 +861,7 @@ def find_groundstate(psi0, H: SparseIMPO, alg=None, envs: Optional[DMRGCache] = 
 
     ``find_groundstate(H, alg)`` (no state) starts from ``randomimps(phydims(H); D = alg.D)``.
     """
-    if isinstance(psi0, SparseIMPO):  # convenience form (vumps.jl:330-336)
+    if isinstance(psi0, SparseIMPO):  # convenience form (vumps.jl:96-101)
         H, alg = psi0, H
         psi0 = randomimps(H.phydims(), D=alg.D, seed=0)
     if which != "SR":

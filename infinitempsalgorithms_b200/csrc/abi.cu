@@ -124,6 +124,9 @@ int imps_ctx_create(int device, imps_ctx** out) {
     IMPS_CUDA(cudaMalloc((void**)&c.dev_info, sizeof(int) * 4));
     cudaDeviceGetAttribute(&c.num_sms, cudaDevAttrMultiProcessorCount, device);
     if (const char* e = std::getenv("IMPS_FP64_ENGINE")) c.fp64_engine = std::atoi(e) == 1 ? 1 : 0;
+    // the allocation-free entry point's fixed array is created with the context,
+    // before the caller's allocator takes the rest of the device memory
+    imps::noalloc_prepare(device);
     return IMPS_OK;
   });
   if (r != IMPS_OK) {

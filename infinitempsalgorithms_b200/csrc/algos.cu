@@ -1,8 +1,8 @@
 // Observables and algorithm steps on the device:
-//   calc_galerkin       (src/algorithms/groundstates/vumps.jl:345-358)
+//   calc_galerkin       (src/algorithms/groundstates/vumps.jl:111-124)
 //   Schur energy        (src/observables/expval.jl:93-112)
 //   local expectation   (expval.jl:33-37)
-//   localupdate_step!   (vumps.jl:241-253), one VUMPS iteration (vumps.jl:296-318)
+//   localupdate_step!   (vumps.jl:7-19), one VUMPS iteration (vumps.jl:51-85)
 //   TDVP timestep       (src/algorithms/timeevo/tdvp.jl:34-53)
 //   IDMRG sweep         (src/algorithms/groundstates/idmrg.jl:12-33)
 #include "algos.h"

@@ -1,7 +1,7 @@
 // Gauge fixing on the device: uniform_leftorth! / uniform_rightorth!
 // (src/states/ortho.jl:125-202), regauge! (:214-219), the CanonicalIMPS
 // constructors (src/states/canonicalmps.jl:151-195), gauge_step!
-// (src/algorithms/groundstates/vumps.jl:257-266) and dot(psi, psi)
+// (src/algorithms/groundstates/vumps.jl:23-31) and dot(psi, psi)
 // (canonicalmps.jl:262-269).  All factorizations are FP64 QRpos / LQpos.
 #include "gauge.h"
 

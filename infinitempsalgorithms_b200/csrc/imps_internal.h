@@ -358,6 +358,8 @@ void push_right_levels(Context* ctx, const MpoSite& W, int Dl, int d, int Dr, co
 void ac_apply_noalloc(Context* ctx, int Dl, int d, int Dr, int m, int n, const cplx* W_host, const dcplx* GL,
                       const dcplx* GR, const dcplx* x, dcplx* y);
 size_t noalloc_scratch_bytes();
+// Loads the no-alloc array on `device` (current) and caches its address.
+void noalloc_prepare(int device);
 // Full MPO pushes (transfer_leftenv!/transfer_rightenv!)
 void push_mpo_left(Context* ctx, const MpoSite& W, int Dl, int d, int Dr, const dcplx* L, const dcplx* A, dcplx* out);
 void push_mpo_right(Context* ctx, const MpoSite& W, int Dl, int d, int Dr, const dcplx* R, const dcplx* A,

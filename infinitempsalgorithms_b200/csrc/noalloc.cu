@@ -12,13 +12,22 @@
 //
 // Limits and sharing rules (also stated in include/imps_b200.h):
 //  * the array is kNoAllocScratchBytes (64 MiB) on every device that loads the
-//    library, held until the process exits;
+//    library, held until the process exits.  This file is its own CUDA module, and
+//    with lazy module loading the array comes into being when its address is
+//    first looked up; imps_ctx_create does that lookup (noalloc_prepare), so the
+//    array exists as soon as a context is created on the device, before the
+//    caller's allocator reserves the rest of the memory;
 //  * the intermediates need 16 * Dl * d * Dr * (m + n) bytes plus the MPO
 //    tensor (at most 64 KiB); larger problems are rejected with IMPS_INVALID_ARG;
 //  * every call uses the same array and leaves its contents behind, so calls
 //    whose GPU work overlaps (other streams, other host threads) race;
-//  * the first call on a device looks up the array's device address
-//    (cudaGetSymbolAddress); make that first call before any stream capture.
+//  * the call is asynchronous: its work is queued on the context's stream, which
+//    the caller orders against its own producers and consumers of GL, GR, x, y
+//    (or shares through imps_ctx_set_stream);
+//  * W_host is copied into the array during the call.
+#include <atomic>
+#include <mutex>
+
 #include "imps_internal.h"
 
 namespace imps {
@@ -33,19 +42,26 @@ constexpr size_t kNoAllocWBytes = size_t(64) << 10;
 __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
 constexpr int kMaxDevices = 64;
-void* g_scratch_addr[kMaxDevices] = {nullptr};
+// Per-device address of the array.  Contexts on several host threads may look it
+// up at the same time: the lookup itself runs under a mutex and the published
+// pointer is atomic.
+std::atomic<void*> g_scratch_addr[kMaxDevices];
+std::mutex g_scratch_mu;
 
 // Once per device, with that device current: the array's device address.
 void* scratch_address(int device) {
   IMPS_REQUIRE(device >= 0 && device < kMaxDevices, IMPS_INVALID_ARG, "device ordinal out of range");
-  if (!g_scratch_addr[device]) {
-    void* p = nullptr;
+  void* p = g_scratch_addr[device].load(std::memory_order_acquire);
+  if (p) return p;
+  std::lock_guard<std::mutex> lock(g_scratch_mu);
+  p = g_scratch_addr[device].load(std::memory_order_relaxed);
+  if (!p) {
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     IMPS_REQUIRE(e == cudaSuccess && p != nullptr, IMPS_CUDA_ERROR,
                  std::string("cudaGetSymbolAddress(no-alloc scratch): ") + cudaGetErrorString(e));
-    g_scratch_addr[device] = p;
+    g_scratch_addr[device].store(p, std::memory_order_release);
   }
-  return g_scratch_addr[device];
+  return p;
 }
 
 // Disables the per-kernel event timers (they create CUDA events) for one call.
@@ -112,5 +128,7 @@ void ac_apply_noalloc(Context* ctx, int Dl, int d, int Dr, int m, int n, const c
 }
 
 size_t noalloc_scratch_bytes() { return kNoAllocScratchBytes - kNoAllocWBytes; }
+
+void noalloc_prepare(int device) { (void)scratch_address(device); }
 
 }  // namespace imps

@@ -12,7 +12,7 @@ Parity status
   absent).  Every function below restates the cited reference lines.
 * Pinned against the reference's own known-answer tests (``tests/test_oracle.py``):
   TFIM ``e0 = -4/pi`` (``test/algorithms/vumps.jl:15-18``), XXZ
-  ``e0 = 1/4 - ln 2`` (``vumps.jl:7-12``), the N=1 TFIM Galerkin < 1e-9 run
+  ``e0 = 1/4 - ln 2`` (``test/algorithms/vumps.jl:7-12``), the N=1 TFIM Galerkin < 1e-9 run
   (``test/algorithms/api.jl:481-489``), Heff Hermiticity and identity
   (``api.jl:226-239``), ``regularize!`` (``api.jl:243-246``), ``linsolve``
   coefficients (``api.jl:248-251``), ``contract_mpo_expval``
@@ -1264,7 +1264,7 @@ def _eig_params(alg):
 
 def find_groundstate(psi0: CanonicalIMPS, H: SchurMPO, alg: VUMPS, envs: Optional[DMRGCache] = None,
                      log: Optional[list] = None):
-    """``find_groundstate(psi0, H, ::VUMPS)`` (``src/algorithms/groundstates/vumps.jl:285-320``).
+    """``find_groundstate(psi0, H, ::VUMPS)`` (``src/algorithms/groundstates/vumps.jl:51-85``).
 
     Returns ``(psi, envs, info)`` with ``info = dict(niter, converged, losses, itererr)``.
     """
@@ -1307,7 +1307,7 @@ def find_groundstate(psi0: CanonicalIMPS, H: SchurMPO, alg: VUMPS, envs: Optiona
 
 
 def canonical_from_AL_keepAL(ALs, C0, tol, maxiter) -> CanonicalIMPS:
-    """``gauge_step!`` (``vumps.jl:257-266``): keep the candidate ``AL``, right gauge fix
+    """``gauge_step!`` (``vumps.jl:23-31``): keep the candidate ``AL``, right gauge fix
     from ``C0`` for ``AR, C``, then ``AC = AL C``."""
     psi = gaugefix(ALs, C0, order="R", tol=tol, maxiter=maxiter)
     psi.AC = [_mulAL(psi.AL[i], psi.C[i]) for i in range(len(ALs))]

@@ -48,17 +48,23 @@ def _regular(ctx, W, GL, GR, x):
 
 
 def _noalloc(ctx, W, GL, GR, x):
+    """Returns (y, device bytes the library took during the call)."""
     m, d, n = W.shape[0], W.shape[1], W.shape[2]
     D = x.shape[0]
     Wh = np.asfortranarray(W.astype(complex))
     gl, gr, xd = _dev(GL), _dev(GR), _dev(x)
     yd = torch.zeros_like(xd)
+    # the library queues its work on the context's stream: the caller's fills and
+    # copies above (torch's stream) must be complete before the call reads them
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
     st = ctx.lib.imps_ac_apply_noalloc(ctx.h, D, d, D, m, n, Wh.ctypes.data_as(L.DP), C.c_void_p(gl.data_ptr()),
                                        C.c_void_p(gr.data_ptr()), C.c_void_p(xd.data_ptr()),
                                        C.c_void_p(yd.data_ptr()))
     L.check(st, ctx.h)
-    torch.cuda.synchronize()
-    return yd.cpu().numpy().reshape(x.shape, order="F")
+    ctx.synchronize()
+    free1 = torch.cuda.mem_get_info()[0]
+    return yd.cpu().numpy().reshape(x.shape, order="F"), free0 - free1
 
 
 def test_noalloc_matches_regular_entry_point_twice():
@@ -69,8 +75,13 @@ def test_noalloc_matches_regular_entry_point_twice():
     for seed, D, W in ((1, 24, W1), (2, 40, W2)):
         GL, GR, x = _case(seed, D, W)
         y_ref = _regular(ctx, W, GL, GR, x)
-        y = _noalloc(ctx, W, GL, GR, x)
+        y, _ = _noalloc(ctx, W, GL, GR, x)
         assert np.linalg.norm(y - y_ref) <= 1e-12 * np.linalg.norm(y_ref)
+    # once its kernels are loaded, a call must leave the device's free memory where
+    # it was: nothing is allocated behind the caller's back
+    y, took = _noalloc(ctx, W, GL, GR, x)
+    assert np.linalg.norm(y - y_ref) <= 1e-12 * np.linalg.norm(y_ref)
+    assert took == 0
     ctx.close()
 
 
