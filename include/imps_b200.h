@@ -106,6 +106,23 @@ int imps_ctx_set_stream(imps_ctx* ctx, void* cuda_stream);
  * selects slices per call from the requested solver tolerance. */
 int imps_ctx_set_precision(imps_ctx* ctx, int mode, int nslices);
 int imps_ctx_synchronize(imps_ctx* ctx);
+/* Bound of each pipeline wait inside the split GEMM kernel, in SM clock cycles
+ * (0 restores the default 2e9, about 1 s).  A wait that runs out sets a device
+ * error flag and the kernel returns early; the flag is read at the context's next
+ * host synchronisation (at the latest when the entry point returns) and the call
+ * returns IMPS_TIMEOUT; the context stays usable.  No reference counterpart (the
+ * reference has no device code): the bounded-wait failure detection of this
+ * library. */
+int imps_ctx_set_wait_limit(imps_ctx* ctx, int64_t cycles);
+/* Cap (bytes, 0 = none) on the context's scratch workspace: the grow-only device
+ * buffers the solvers and contractions keep between calls (Krylov bases, Heff
+ * intermediates, gauge work arrays).  A call that would grow it past the cap
+ * returns IMPS_OOM and leaves the context usable; imps_ctx_workspace_bytes reports
+ * the current size.  Object storage (states, environments, MPOs) and the cached
+ * int8 operand splits are not counted.  No reference counterpart (Julia's GC owns
+ * the reference's arrays). */
+int imps_ctx_set_workspace_limit(imps_ctx* ctx, int64_t bytes);
+int imps_ctx_workspace_bytes(imps_ctx* ctx, int64_t* bytes);
 const char* imps_ctx_last_error(const imps_ctx* ctx);
 const char* imps_status_string(int status);
 /* Kernel timing with CUDA events on the context stream, per kernel class. */
@@ -121,6 +138,10 @@ int imps_ctx_profile_dump(imps_ctx* ctx, char* buf, int64_t len);
  * QRpos/LQpos factorizations, real flops of all complex GEMMs (8 M N K each), real flops of
  * the QR factorizations */
 int imps_ctx_counters(imps_ctx* ctx, int64_t* counters);
+/* The same counters followed by [8] split GEMM launches, [9] their algorithmic real
+ * flops (8 M N K of each complex product) and [10] the int8 operations the tensor
+ * pipe executed for them; n entries are written (entries past 10 read 0). */
+int imps_ctx_counters_ext(imps_ctx* ctx, int64_t* counters, int n);
 
 /* -------------------------------------------------------------------- MPO */
 /* Replaces SparseIMPO / SchurMPOTensor storage (src/operators/mpohamiltonian.jl:33-52):

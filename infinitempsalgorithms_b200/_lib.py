@@ -79,6 +79,10 @@ _SIGS = {
     "imps_ctx_set_stream": (I32, [P, P]),
     "imps_ctx_set_precision": (I32, [P, I32, I32]),
     "imps_ctx_synchronize": (I32, [P]),
+    "imps_ctx_set_wait_limit": (I32, [P, I64]),
+    "imps_ctx_set_workspace_limit": (I32, [P, I64]),
+    "imps_ctx_workspace_bytes": (I32, [P, C.POINTER(I64)]),
+    "imps_ctx_counters_ext": (I32, [P, C.POINTER(I64), I32]),
     "imps_ctx_last_error": (C.c_char_p, [P]),
     "imps_ctx_profile": (I32, [P, I32]),
     "imps_ctx_profile_get": (I32, [P, C.c_char_p, C.POINTER(I64), DP, DP]),

@@ -157,10 +157,11 @@ class Context:
         return out
 
     def counters(self):
-        arr = (C.c_int64 * 8)()
-        check(self.lib.imps_ctx_counters(self.h, arr), self.h)
+        arr = (C.c_int64 * 11)()
+        check(self.lib.imps_ctx_counters_ext(self.h, arr, 11), self.h)
         return dict(ac_apply=arr[0], c_apply=arr[1], push=arr[2], gemm=arr[3], kernels=arr[4], qr=arr[5],
-                    gemm_flops=arr[6], qr_flops=arr[7])
+                    gemm_flops=arr[6], qr_flops=arr[7], split_launches=arr[8], split_alg_flops=arr[9],
+                    split_exec_ops=arr[10])
 
     def close(self):
         """Destroy the context; device objects created on it are released first."""

@@ -28,6 +28,8 @@ int guard(imps::Context* ctx, F&& f) {
   try {
     if (ctx) cudaSetDevice(ctx->device);
     int r = f();
+    // a bounded wait that ran out inside this call surfaces here at the latest
+    if (ctx) imps::check_device_errors(ctx);
     return r;
   } catch (const imps::Error& e) {
     g_last_error = e.what();
@@ -122,6 +124,10 @@ int imps_ctx_create(int device, imps_ctx** out) {
     IMPS_SOLVER(cusolverDnCreate(&c.solver));
     IMPS_SOLVER(cusolverDnSetStream(c.solver, c.stream));
     IMPS_CUDA(cudaMalloc((void**)&c.dev_info, sizeof(int) * 4));
+    IMPS_CUDA(cudaMalloc((void**)&c.err_dev, sizeof(int) * 4));
+    IMPS_CUDA(cudaMemset(c.err_dev, 0, sizeof(int) * 4));
+    IMPS_CUDA(cudaMallocHost((void**)&c.err_host, sizeof(int) * 4));
+    c.err_host[0] = 0;
     cudaDeviceGetAttribute(&c.num_sms, cudaDevAttrMultiProcessorCount, device);
     if (const char* e = std::getenv("IMPS_FP64_ENGINE")) c.fp64_engine = std::atoi(e) == 1 ? 1 : 0;
     // the allocation-free entry point's fixed array is created with the context,
@@ -151,6 +157,8 @@ int imps_ctx_destroy(imps_ctx* h) {
   c.red.release();
   if (c.host_pinned) cudaFreeHost(c.host_pinned);
   if (c.dev_info) cudaFree(c.dev_info);
+  if (c.err_dev) cudaFree(c.err_dev);
+  if (c.err_host) cudaFreeHost(c.err_host);
   if (c.solver) cusolverDnDestroy(c.solver);
   if (c.own_stream && c.stream) cudaStreamDestroy(c.stream);
   delete h;
@@ -187,6 +195,36 @@ int imps_ctx_synchronize(imps_ctx* h) {
     IMPS_CUDA(cudaStreamSynchronize(h->c.stream));
     return IMPS_OK;
   });
+}
+
+int imps_ctx_set_wait_limit(imps_ctx* h, int64_t cycles) {
+  if (!h || cycles < 0) return IMPS_INVALID_ARG;
+  h->c.wait_cycles = cycles > 0 ? (long long)cycles : 2000000000LL;
+  return IMPS_OK;
+}
+
+int imps_ctx_set_workspace_limit(imps_ctx* h, int64_t bytes) {
+  if (!h || bytes < 0) return IMPS_INVALID_ARG;
+  h->c.workspace_limit = (size_t)bytes;
+  return IMPS_OK;
+}
+
+int imps_ctx_workspace_bytes(imps_ctx* h, int64_t* bytes) {
+  if (!h || !bytes) return IMPS_INVALID_ARG;
+  size_t total = 0;
+  for (const auto& kv : h->c.scratch) total += kv.second.bytes;
+  *bytes = (int64_t)total;
+  return IMPS_OK;
+}
+
+int imps_ctx_counters_ext(imps_ctx* h, int64_t* c, int n) {
+  if (!h || !c || n < 0) return IMPS_INVALID_ARG;
+  const imps::Context& x = h->c;
+  const int64_t all[11] = {x.n_ac_apply, x.n_c_apply, x.n_push, x.n_gemm, x.n_kernels, x.n_qr,
+                           (int64_t)x.gemm_flops, (int64_t)x.qr_flops, x.split_launches,
+                           (int64_t)x.split_alg_flops, (int64_t)x.split_exec_ops};
+  for (int i = 0; i < n; ++i) c[i] = i < 11 ? all[i] : 0;
+  return IMPS_OK;
 }
 
 const char* imps_ctx_last_error(const imps_ctx* h) {

@@ -28,8 +28,12 @@
 //           TMEM, so the epilogue of one tile overlaps the MMAs of the next.
 // The K extent is cut into groups so that no int32 sum can overflow: the largest
 // diagonal adds s pairs, so a group spans fewer than 2^31 / (127^2 s) bytes.
-// Every mbarrier wait is bounded (~1 s of clock64); on expiry the kernel sets an
-// error flag, drains and returns, and the host raises IMPS_TIMEOUT.
+// Every mbarrier wait of the pipeline is bounded (GemmArgs::wait_cycles of clock64,
+// ~1 s by default); on expiry the kernel sets the context's error flag, waits (with a
+// fixed ~1 s bound) for the copies and MMAs it has in flight, frees its TMEM and
+// returns.  The flag is read back at the next host synchronisation of the context
+// and raised as IMPS_TIMEOUT; a set flag also makes every later pipeline wait give
+// up at once, so the rest of the failing call costs little.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -57,7 +61,7 @@ constexpr int B_TILE = BN * KB;  // 4 KB per slice
 constexpr int STAGE_BUDGET = 200 * 1024;
 constexpr int BAR_BYTES = 512;
 constexpr int NTHREADS = 32 * (2 + EPI_WARPS);
-constexpr long long WAIT_CYCLES = 2000000000LL;   // ~1 s at 1.9 GHz
+constexpr long long DRAIN_CYCLES = 2000000000LL;  // ~1 s at 1.9 GHz: bound of the error-path drains
 
 __host__ __device__ constexpr int stages_for(int s) {
   return (STAGE_BUDGET / (s * (A_TILE + B_TILE))) < MAX_STAGES ? (STAGE_BUDGET / (s * (A_TILE + B_TILE)))
@@ -97,17 +101,18 @@ __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// bounded wait: returns false (and raises the error flag) after ~1 s.  The fast path
-// only polls the barrier; the global error flag and the clock are checked every
-// 256 unsuccessful polls so a completed phase is seen without extra memory latency.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* err) {
+// bounded wait: returns false (and raises the error flag) after `limit` cycles.  The
+// fast path only polls the barrier; the global error flag and the clock are checked
+// every 256 unsuccessful polls so a completed phase is seen without extra memory
+// latency.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* err, long long limit) {
   if (mbar_try(bar, parity)) return true;
   const long long t0 = clock64();
   unsigned spins = 0;
   while (!mbar_try(bar, parity)) {
     if ((++spins & 255u) != 0u) continue;
     if (*err) return false;
-    if (clock64() - t0 > WAIT_CYCLES) {
+    if (clock64() - t0 > limit) {
       atomicExch((int*)err, 1);
       return false;
     }
@@ -182,6 +187,7 @@ struct GemmArgs {
   double alpha;
   int accumulate;            // 0: C = result, 1: C += result
   int* err;
+  long long wait_cycles;     // bound of each pipeline wait (SM clock cycles)
 };
 
 // Accumulation groups of one tile: K range [kb0, kb1) of every slice pair; the
@@ -276,7 +282,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         int mb, nb;
         tile_coords(g, t, mb, nb);
         for (int kb = 0; kb < g.kblocks && ok; ++kb) {
-          ok = mbar_wait(&empty[stage], phase ^ 1, err);
+          ok = mbar_wait(&empty[stage], phase ^ 1, err, g.wait_cycles);
           if (!ok) break;
           uint8_t* base = smem + stage * stage_bytes;
           mbar_expect_tx(&full[stage], (uint32_t)stage_bytes);
@@ -292,7 +298,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       for (int s2 = 0; s2 < NST; ++s2) {
         if (issued[s2] < 0) continue;
         long long t0 = clock64();
-        while (!mbar_try(&full[s2], (uint32_t)issued[s2]) && clock64() - t0 < WAIT_CYCLES) {
+        while (!mbar_try(&full[s2], (uint32_t)issued[s2]) && clock64() - t0 < DRAIN_CYCLES) {
         }
       }
     }
@@ -306,12 +312,12 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
         for (GroupIter gi(&g); gi.valid() && ok; gi.next(), ++grp) {
           const int buf = grp % NBUF;
-          ok = mbar_wait(&tempty[buf], ((grp / NBUF) & 1) ^ 1, err);
+          ok = mbar_wait(&tempty[buf], ((grp / NBUF) & 1) ^ 1, err, g.wait_cycles);
           if (!ok) break;
           tc_fence_after();
           const int kb1 = gi.kb1();
           for (int kb = gi.kb0; kb < kb1 && ok; ++kb) {
-            ok = mbar_wait(&full[stage], phase, err);
+            ok = mbar_wait(&full[stage], phase, err, g.wait_cycles);
             if (!ok) break;
             tc_fence_after();
             const uint32_t a0 = smem_u32(smem + stage * stage_bytes);
@@ -328,7 +334,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       // all MMAs issued by this thread retire before TMEM is released (bounded)
       umma_commit(drain);
       long long t0 = clock64();
-      while (!mbar_try(drain, 0) && clock64() - t0 < WAIT_CYCLES) {
+      while (!mbar_try(drain, 0) && clock64() - t0 < DRAIN_CYCLES) {
       }
     }
   } else {
@@ -349,7 +355,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       bool ok = true;
       for (GroupIter gi(&g); gi.valid(); gi.next(), ++grp) {
         const int buf = grp % NBUF;
-        if (!mbar_wait(&tfull[buf], (grp / NBUF) & 1, err)) { ok = false; break; }
+        if (!mbar_wait(&tfull[buf], (grp / NBUF) & 1, err, g.wait_cycles)) { ok = false; break; }
         tc_fence_after();
         for (int d = 0; d < S; ++d) {
           const double w = ldexp(1.0, -7 * (d + 2));
@@ -683,8 +689,6 @@ void split_gemm(Context* ctx, const SplitOperand& A, const SplitOperand& B, int 
   }
   const CUtensorMap mapA = make_map(static_cast<const int8_t*>(A.data.ptr), A.Kp, A.Rp, A.s, BM);
   const CUtensorMap mapB = make_map(static_cast<const int8_t*>(B.data.ptr), B.Kp, B.Rp, B.s, BN);
-  DevBuf& errb = ctx->buf("gemm_i8_err", 16);
-  IMPS_CUDA(cudaMemsetAsync(errb.ptr, 0, 16, ctx->stream));
   GemmArgs g;
   g.num_m = (int)(A.Rp / BM);
   g.num_n = (int)(B.Rp / BN);
@@ -702,7 +706,8 @@ void split_gemm(Context* ctx, const SplitOperand& A, const SplitOperand& B, int 
   g.col_scale = B.scale.d();
   g.alpha = alpha;
   g.accumulate = accumulate ? 1 : 0;
-  g.err = static_cast<int*>(errb.ptr);
+  g.err = ctx->err_dev;
+  g.wait_cycles = ctx->wait_cycles;
   const int ntiles = g.num_m * g.num_n;
   const int grid = std::max(1, std::min(ntiles, ctx->num_sms));
   {
@@ -720,10 +725,11 @@ void split_gemm(Context* ctx, const SplitOperand& A, const SplitOperand& B, int 
     ctx->n_gemm++;
     IMPS_CUDA(cudaPeekAtLastError());
   }
-  int herr = 0;
-  IMPS_CUDA(cudaMemcpyAsync(&herr, errb.ptr, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-  IMPS_CUDA(cudaStreamSynchronize(ctx->stream));
-  IMPS_REQUIRE(herr == 0, IMPS_TIMEOUT, "split GEMM: a pipeline wait timed out");
+  ctx->split_launches++;
+  ctx->split_alg_flops += 8.0 * (double)A.rows * (double)B.rows * (double)A.K;
+  ctx->split_exec_ops += 2.0 * (double)A.Rp * (double)B.Rp * (double)A.Kp * (double)(s * (s + 1) / 2);
+  // the error flag is read at the context's next host synchronisation
+  ctx->err_armed = true;
 }
 
 }  // namespace imps

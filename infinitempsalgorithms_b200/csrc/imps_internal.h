@@ -118,6 +118,12 @@ struct Context {
   double* host_pinned = nullptr;
   size_t host_pinned_bytes = 0;
   int* dev_info = nullptr;
+  // device error flag of the bounded waits (split GEMM) and its pinned host copy;
+  // armed while a kernel that may set it has not been checked at a synchronisation
+  int* err_dev = nullptr;
+  int* err_host = nullptr;
+  bool err_armed = false;
+  long long wait_cycles = 2000000000LL;  // bound of each pipeline wait (~1 s at 1.9 GHz)
   // profiling
   bool profile = false;
   const char* prof_tag = "";           // call-site tag appended to kernel classes when profiling
@@ -139,9 +145,22 @@ struct Context {
   std::map<SplitKey, std::shared_ptr<SplitOperand>> split_cache;
   std::shared_ptr<SplitOperand> split_scratch[2];
   int64_t split_calls = 0, split_cache_hits = 0;
+  // split GEMM launches, their algorithmic work (8 M N K real flops of the complex
+  // product each computes) and the int8 operations the tensor pipe executes for it
+  int64_t split_launches = 0;
+  double split_alg_flops = 0.0, split_exec_ops = 0.0;
 
+  // cap on the named scratch workspace below (0 = none); growing past it is IMPS_OOM
+  size_t workspace_limit = 0;
   DevBuf& buf(const std::string& name, size_t bytes) {
     DevBuf& b = scratch[name];
+    if (bytes > b.bytes && workspace_limit > 0) {
+      size_t total = 0;
+      for (const auto& kv : scratch) total += kv.second.bytes;
+      if (total - b.bytes + bytes > workspace_limit)
+        throw Error(IMPS_OOM, "workspace limit of " + std::to_string(workspace_limit) + " bytes reached (buffer '" +
+                                  name + "' needs " + std::to_string(bytes) + " bytes)");
+    }
     b.ensure(bytes);
     return b;
   }
@@ -325,6 +344,10 @@ void zcopy2d(Context* ctx, int rows, int cols, const dcplx* X, int64_t ldx, dcpl
 // Q overwrites nothing: results go to Q (m x k) and R (k x n), k = min(m, n).
 void qrpos(Context* ctx, int m, int n, const dcplx* M, int64_t ldm, dcplx* Q, dcplx* R);
 void lqpos(Context* ctx, int m, int n, const dcplx* M, int64_t ldm, dcplx* L, dcplx* Q);
+
+// Reads the device error flag if a kernel that may set it ran since the last check
+// (synchronises the stream); a set flag is cleared and raised as IMPS_TIMEOUT.
+void check_device_errors(Context* ctx);
 
 // Host <-> device
 void upload(Context* ctx, void* dst, const void* src, size_t bytes);

@@ -325,15 +325,40 @@ ScopedTimer::~ScopedTimer() {
   }
 }
 
+// The error flag rides along with a synchronisation that happens anyway.
+static void err_copy(Context* ctx) {
+  if (ctx->err_armed)
+    IMPS_CUDA(cudaMemcpyAsync(ctx->err_host, ctx->err_dev, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+}
+static void err_after_sync(Context* ctx) {
+  if (!ctx->err_armed) return;
+  ctx->err_armed = false;
+  if (ctx->err_host[0] != 0) {
+    ctx->err_host[0] = 0;
+    IMPS_CUDA(cudaMemsetAsync(ctx->err_dev, 0, sizeof(int), ctx->stream));
+    throw Error(IMPS_TIMEOUT, "a bounded device wait of the split GEMM pipeline ran out");
+  }
+}
+void check_device_errors(Context* ctx) {
+  if (!ctx->err_armed) return;
+  err_copy(ctx);
+  IMPS_CUDA(cudaStreamSynchronize(ctx->stream));
+  err_after_sync(ctx);
+}
+
 void upload(Context* ctx, void* dst, const void* src, size_t bytes) {
   if (!bytes) return;
   IMPS_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  err_copy(ctx);
   IMPS_CUDA(cudaStreamSynchronize(ctx->stream));
+  err_after_sync(ctx);
 }
 void download(Context* ctx, void* dst, const void* src, size_t bytes) {
   if (!bytes) return;
   IMPS_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  err_copy(ctx);
   IMPS_CUDA(cudaStreamSynchronize(ctx->stream));
+  err_after_sync(ctx);
 }
 
 void zcopy(Context* ctx, int64_t n, const dcplx* x, dcplx* y) {
