@@ -327,6 +327,12 @@ cplx zdotc(Context* ctx, int64_t n, const dcplx* x, const dcplx* y);  // sum con
 // is given, ||w_old||^2.
 double proj_pass(Context* ctx, int64_t n, int nv, const dcplx* V, int64_t ldv, dcplx* w, cplx* h_host,
                  double* nw_old2);
+// Classical Gram-Schmidt with iterative refinement of w against the nv columns of V
+// (KrylovKit's ClassicalGramSchmidtIR, eta = 1/sqrt(2), at most three projections):
+// h (host) receives the accumulated coefficients; returns the final ||w||.  Each
+// update is fused with the next projection's dots, one host synchronisation per
+// projection after the first.  A non-finite norm raises IMPS_INVALID_ARG.
+double gs_project(Context* ctx, int64_t n, int nv, const dcplx* V, int64_t ldv, dcplx* w, std::vector<cplx>& h);
 // w += sum_j coef[j] V[:, j]
 void zgemv_acc(Context* ctx, int64_t n, int nv, const dcplx* V, int64_t ldv, const cplx* coef, dcplx* w);
 // y = sum_j coef[j] V[:, j]

@@ -23,18 +23,7 @@ namespace {
 // repeated while it shrank ||w|| below eta times its previous value (at most three
 // passes).  Returns the accumulated coefficients (host) and the final ||w||.
 double cgs2(Context* ctx, int64_t n, int nv, const dcplx* V, dcplx* w, std::vector<cplx>& h) {
-  h.assign(nv, cplx(0.0, 0.0));
-  if (nv == 0) return dznrm2(ctx, n, w);
-  std::vector<cplx> h1(nv);
-  double nw0 = 0.0;
-  double nw1 = proj_pass(ctx, n, nv, V, n, w, h1.data(), &nw0);
-  for (int j = 0; j < nv; ++j) h[j] += h1[j];
-  for (int pass = 1; pass < 3 && nw1 < 0.5 * nw0; ++pass) {
-    nw0 = nw1;
-    nw1 = proj_pass(ctx, n, nv, V, n, w, h1.data(), nullptr);
-    for (int j = 0; j < nv; ++j) h[j] += h1[j];
-  }
-  return std::sqrt(std::max(nw1, 0.0));
+  return gs_project(ctx, n, nv, V, n, w, h);
 }
 
 std::vector<cplx> herm_part(const std::vector<cplx>& H, int ldh, int m) {
@@ -62,6 +51,7 @@ KrylovResult lanczos_eigsolve(Context* ctx, int64_t n, const LinOp& A, const dcp
   DevBuf& X0 = ctx->buf("kry_x0", (size_t)n * sizeof(dcplx));
   dcplx* V = Vb.z();
   double beta0 = dznrm2(ctx, n, x0);
+  IMPS_REQUIRE(std::isfinite(beta0), IMPS_INVALID_ARG, "eigsolve: the starting vector holds NaN or Inf");
   IMPS_REQUIRE(beta0 > 0, IMPS_INVALID_ARG, "eigsolve: zero starting vector");
   zaxpby(ctx, n, 1.0 / beta0, x0, 0.0, X0.z());
   zcopy(ctx, n, X0.z(), V);
@@ -281,12 +271,18 @@ KrylovResult exponentiate(Context* ctx, int64_t n, const LinOp& A, cplx t, const
 
 KrylovResult arnoldi_dominant(Context* ctx, int64_t n, const LinOp& A, const dcplx* x0, dcplx* x, double tol,
                               int krylovdim, int maxiter, bool eager) {
+  // Krylov-Schur form A V[:, :m] = V[:, :m+1] H[:m+1, :m], with H upper Hessenberg
+  // apart from the leading keep x keep Schur block and its coupling row after a
+  // restart.  A full basis restarts from the leading `keep` Schur vectors of
+  // H[:m, :m] (ordered by |lambda|) plus the residual vector, which keeps the
+  // subspace of the dominant Ritz values (KrylovKit's schursolve restart).
   KrylovResult res;
   const int kdim = (int)std::min<int64_t>(krylovdim, n);
   DevBuf& Vb = ctx->buf("arn_V", (size_t)n * (kdim + 1) * sizeof(dcplx));
   DevBuf& X0 = ctx->buf("arn_x0", (size_t)n * sizeof(dcplx));
   dcplx* V = Vb.z();
   double nx0 = dznrm2(ctx, n, x0);
+  IMPS_REQUIRE(std::isfinite(nx0), IMPS_INVALID_ARG, "arnoldi: the starting vector holds NaN or Inf");
   IMPS_REQUIRE(nx0 > 0, IMPS_INVALID_ARG, "arnoldi: zero starting vector");
   zaxpby(ctx, n, 1.0 / nx0, x0, 0.0, X0.z());
   zcopy(ctx, n, X0.z(), V);
@@ -312,7 +308,10 @@ KrylovResult arnoldi_dominant(Context* ctx, int64_t n, const LinOp& A, const dcp
       if (std::abs(lam[j]) > std::abs(lam[jd])) jd = j;
     std::vector<cplx> y(m);
     for (int i = 0; i < m; ++i) y[i] = Y[i + (size_t)m * jd];
-    double rnorm = std::abs(hn * y[m - 1]);
+    // residual of the Ritz pair: |row m of H . y| times the unit residual vector
+    cplx ry = 0.0;
+    for (int j = 0; j < m; ++j) ry += H[m + (size_t)ldh * j] * y[j];
+    const double rnorm = std::abs(ry);
     const bool breakdown = hn <= 1e-14 * std::max(1.0, std::abs(lam[jd]));
     const bool full = (m == kdim);
     auto ritz = [&]() {
@@ -331,15 +330,34 @@ KrylovResult arnoldi_dominant(Context* ctx, int64_t n, const LinOp& A, const dcp
       }
     }
     if (full) {
-      ritz();
       if (res.numiter >= maxiter) {
+        ritz();
         res.normres = rnorm;
         res.value = lam[jd];
         return res;
       }
-      zcopy(ctx, n, x, V);
-      std::fill(H.begin(), H.end(), cplx(0.0, 0.0));
-      nvec = 1;
+      // Krylov-Schur restart
+      std::vector<cplx> T, Z;
+      schur_sorted(m, Hm, T, Z);
+      const int nconv = rnorm <= tol ? 1 : 0;
+      const int keep = std::max(1, std::min(m - 1, (3 * kdim + 2 * nconv) / 5));
+      DevBuf& Tb = ctx->buf("arn_tmp", (size_t)n * keep * sizeof(dcplx));
+      DevBuf& Zd = ctx->buf("arn_Z", (size_t)m * keep * sizeof(dcplx));
+      upload(ctx, Zd.ptr, Z.data(), (size_t)m * keep * sizeof(dcplx));
+      zgemm_fp64(ctx, OP_N, OP_N, (int)n, keep, m, 1.0, V, n, 0, Zd.z(), m, 0, 0.0, Tb.z(), n, 0, 1);
+      // residual direction (unit after scaling) moves to slot `keep`
+      zscal(ctx, n, 1.0 / hn, w);
+      zcopy(ctx, n, w, V + n * (int64_t)keep);
+      zcopy(ctx, n * keep, Tb.z(), V);
+      std::vector<cplx> Hn((size_t)ldh * kdim, 0.0);
+      for (int j = 0; j < keep; ++j) {
+        for (int i = 0; i <= j; ++i) Hn[i + (size_t)ldh * j] = T[i + (size_t)m * j];
+        cplx bcoef = 0.0;
+        for (int l = 0; l < m; ++l) bcoef += H[m + (size_t)ldh * l] * Z[l + (size_t)m * j];
+        Hn[keep + (size_t)ldh * j] = bcoef;
+      }
+      H.swap(Hn);
+      nvec = keep + 1;
       res.numiter++;
     } else {
       zscal(ctx, n, 1.0 / hn, w);

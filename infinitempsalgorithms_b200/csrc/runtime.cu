@@ -4,6 +4,8 @@
 #include "imps_internal.h"
 
 #include <algorithm>
+#include <vector>
+#include <cmath>
 #include <cstring>
 
 namespace imps {
@@ -149,6 +151,102 @@ __global__ void k_proj_update(int64_t n, int nv, const dcplx* __restrict__ V, in
     const double r = block_sum<kRedThreads>(nn, sh);
     if (threadIdx.x == 0) npart[blockIdx.x] = r;
   }
+}
+
+// Block reduction of the per-thread dot accumulators acc[0 .. 2 nv) and the norm
+// accumulator into per-block partials part[blockIdx.x + ldp * k] (k < 2 nv: dots,
+// k = 2 nv: norm), in a fixed order (deterministic).  Indices are compile-time so
+// the accumulators stay in registers.
+template <int NV>
+__device__ __forceinline__ void block_reduce_dots(const double (&acc)[2 * NV], double nrm, int nv, double* part,
+                                                  int64_t ldp) {
+  __shared__ double red[kRedThreads / 32][2 * NV + 1];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < 2 * NV; ++k) {
+    if (k < 2 * nv) {
+      double v = acc[k];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+      if (lane == 0) red[wid][k] = v;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) nrm += __shfl_down_sync(0xffffffffu, nrm, o);
+  if (lane == 0) red[wid][2 * NV] = nrm;
+  __syncthreads();
+  for (int k = threadIdx.x; k <= 2 * nv; k += blockDim.x) {
+    const int src = k < 2 * nv ? k : 2 * NV;
+    double sum = 0.0;
+    for (int q = 0; q < kRedThreads / 32; ++q) sum += red[q][src];
+    part[blockIdx.x + ldp * k] = sum;
+  }
+}
+
+// Gram-Schmidt, first projection: partials of h_j = <V_j, w> (j < nv <= NV,
+// columns 2j, 2j+1) and of ||w||^2 (column 2 nv), one read of V and of w.
+template <int NV>
+__global__ void __launch_bounds__(kRedThreads) k_gs_dots(int64_t n, int nv, const dcplx* __restrict__ V, int64_t ldv,
+                                                     const dcplx* __restrict__ w, double* __restrict__ part,
+                                                     int64_t ldp) {
+  double acc[2 * NV];
+  double nrm = 0.0;
+#pragma unroll
+  for (int k = 0; k < 2 * NV; ++k) acc[k] = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const dcplx wi = w[i];
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+      if (j < nv) {
+        const dcplx p = cmulc(V[i + ldv * j], wi);
+        acc[2 * j] += p.x;
+        acc[2 * j + 1] += p.y;
+      }
+    }
+    nrm = fma(wi.x, wi.x, fma(wi.y, wi.y, nrm));
+  }
+  block_reduce_dots<NV>(acc, nrm, nv, part, ldp);
+}
+
+// Gram-Schmidt, fused update: w <- w - V h with h = hdev (interleaved re, im), and
+// in the same pass the partials of the next projection's h'_j = <V_j, w_new> and of
+// ||w_new||^2 (same column layout as k_gs_dots).  The second read of V_j for an
+// element follows the first within the same thread and is served from L1/L2, so
+// an iterative-refinement pass costs one HBM read of V instead of two.
+template <int NV>
+__global__ void __launch_bounds__(kRedThreads) k_gs_update_dots(int64_t n, int nv, const dcplx* __restrict__ V,
+                                                            int64_t ldv, const double* __restrict__ hdev,
+                                                            dcplx* __restrict__ w, double* __restrict__ part,
+                                                            int64_t ldp) {
+  __shared__ double2 c[NV];
+  if (threadIdx.x < nv) c[threadIdx.x] = make_double2(-hdev[2 * threadIdx.x], -hdev[2 * threadIdx.x + 1]);
+  __syncthreads();
+  double acc[2 * NV];
+  double nrm = 0.0;
+#pragma unroll
+  for (int k = 0; k < 2 * NV; ++k) acc[k] = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    dcplx a = w[i];
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+      if (j < nv) {
+        const dcplx p = cmul(c[j], V[i + ldv * j]);
+        a.x += p.x;
+        a.y += p.y;
+      }
+    }
+    w[i] = a;
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+      if (j < nv) {
+        // a second, separate load (not the register copy of the first): keeps the
+        // live registers to the accumulators
+        const dcplx p = cmulc(__ldca(V + i + ldv * j), a);
+        acc[2 * j] += p.x;
+        acc[2 * j + 1] += p.y;
+      }
+    }
+    nrm = fma(a.x, a.x, fma(a.y, a.y, nrm));
+  }
+  block_reduce_dots<NV>(acc, nrm, nv, part, ldp);
 }
 
 struct CoefPack {
@@ -495,6 +593,81 @@ double proj_pass(Context* ctx, int64_t n, int nv, const dcplx* V, int64_t ldv, d
   for (int j = 0; j < nv; ++j) h_host[j] = cplx(hv[2 * j], hv[2 * j + 1]);
   if (nw_old2) *nw_old2 = hv[2 * nv];
   return hv[2 * nv + 1];
+}
+
+namespace {
+template <int NV>
+void launch_gs(Context* ctx, bool update, int nb, int64_t n, int nv, const dcplx* V, int64_t ldv, const double* hdev,
+               dcplx* w, double* part) {
+  if (update)
+    k_gs_update_dots<NV><<<nb, kRedThreads, 0, ctx->stream>>>(n, nv, V, ldv, hdev, w, part, nb);
+  else
+    k_gs_dots<NV><<<nb, kRedThreads, 0, ctx->stream>>>(n, nv, V, ldv, w, part, nb);
+  check_launch(ctx);
+}
+void gs_pass(Context* ctx, bool update, int nb, int64_t n, int nv, const dcplx* V, int64_t ldv, const double* hdev,
+             dcplx* w, double* part, double* out) {
+  if (nv <= 8) launch_gs<8>(ctx, update, nb, n, nv, V, ldv, hdev, w, part);
+  else if (nv <= 16) launch_gs<16>(ctx, update, nb, n, nv, V, ldv, hdev, w, part);
+  else launch_gs<32>(ctx, update, nb, n, nv, V, ldv, hdev, w, part);
+  k_final_sum_cols<<<2 * nv + 1, kRedThreads, 0, ctx->stream>>>(nb, part, nb, out);
+  check_launch(ctx);
+}
+const char* kNonFinite =
+    "non-finite value (NaN or Inf) in the Krylov iteration: the operator or the start vector holds one";
+}  // namespace
+
+double gs_project(Context* ctx, int64_t n, int nv, const dcplx* V, int64_t ldv, dcplx* w, std::vector<cplx>& h) {
+  h.assign(nv, cplx(0.0, 0.0));
+  if (nv <= 0) {
+    const double nw = dznrm2(ctx, n, w);
+    IMPS_REQUIRE(std::isfinite(nw), IMPS_INVALID_ARG, kNonFinite);
+    return nw;
+  }
+  if (nv > 32) {
+    // wide bases: the chunked two-kernel projection
+    std::vector<cplx> h1(nv);
+    double nw0 = 0.0;
+    double nw1 = proj_pass(ctx, n, nv, V, ldv, w, h1.data(), &nw0);
+    IMPS_REQUIRE(std::isfinite(nw0) && std::isfinite(nw1), IMPS_INVALID_ARG, kNonFinite);
+    for (int j = 0; j < nv; ++j) h[j] += h1[j];
+    for (int pass = 1; pass < 3 && nw1 < 0.5 * nw0; ++pass) {
+      nw0 = nw1;
+      nw1 = proj_pass(ctx, n, nv, V, ldv, w, h1.data(), nullptr);
+      for (int j = 0; j < nv; ++j) h[j] += h1[j];
+    }
+    return std::sqrt(std::max(nw1, 0.0));
+  }
+  const int nb = std::min(red_blocks(n), 592);
+  const int ncol = 2 * nv + 1;
+  DevBuf& part = ctx->buf("gs_part", (size_t)nb * ncol * sizeof(double));
+  DevBuf& outb = ctx->buf("gs_out", (size_t)3 * ncol * sizeof(double));
+  double* out[3] = {outb.d(), outb.d() + ncol, outb.d() + 2 * ncol};
+  ScopedTimer t(ctx, "orth", (double)n * 16 * (nv + 1));
+  // projection 1 (dots of w), then its update fused with the dots of projection 2
+  gs_pass(ctx, false, nb, n, nv, V, ldv, nullptr, w, part.d(), out[0]);
+  gs_pass(ctx, true, nb, n, nv, V, ldv, out[0], w, part.d(), out[1]);
+  std::vector<double> hv(2 * ncol);
+  download(ctx, hv.data(), out[0], hv.size() * sizeof(double));
+  double nw0 = hv[2 * nv], nw1 = hv[ncol + 2 * nv];
+  IMPS_REQUIRE(std::isfinite(nw0) && std::isfinite(nw1), IMPS_INVALID_ARG, kNonFinite);
+  for (int j = 0; j < nv; ++j) h[j] = cplx(hv[2 * j], hv[2 * j + 1]);
+  // iterative refinement (KrylovKit's ClassicalGramSchmidtIR, eta = 1/sqrt(2)): apply the
+  // pending projection while the last one shrank ||w|| below eta of its previous value,
+  // at most three projections in all
+  int cur = 1;
+  std::vector<double> hn(hv.begin() + ncol, hv.end());
+  for (int pass = 1; pass < 3 && nw1 < 0.5 * nw0; ++pass) {
+    const int nxt = cur == 1 ? 2 : 1;
+    gs_pass(ctx, true, nb, n, nv, V, ldv, out[cur], w, part.d(), out[nxt]);
+    for (int j = 0; j < nv; ++j) h[j] += cplx(hn[2 * j], hn[2 * j + 1]);
+    download(ctx, hn.data(), out[nxt], ncol * sizeof(double));
+    nw0 = nw1;
+    nw1 = hn[2 * nv];
+    IMPS_REQUIRE(std::isfinite(nw1), IMPS_INVALID_ARG, kNonFinite);
+    cur = nxt;
+  }
+  return std::sqrt(std::max(nw1, 0.0));
 }
 
 void zconj_transpose(Context* ctx, int m, int n, const dcplx* X, int64_t ldx, dcplx* Y, int64_t ldy) {

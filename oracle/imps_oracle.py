@@ -54,7 +54,7 @@ __all__ = [
     "uniform_rightorth", "gaugefix", "regauge", "randomimps", "random_site_tensors",
     "state_dot", "DMRGCache", "build_envs", "ac_apply", "c_apply", "calc_galerkin",
     "expectationvalue", "local_expectation1", "VUMPS", "TDVP", "IDMRG",
-    "find_groundstate", "timestep", "time_evolve", "idmrg_groundstate",
+    "find_groundstate", "vumps_iteration", "timestep", "time_evolve", "idmrg_groundstate",
 ]
 
 C128 = np.complex128
@@ -343,21 +343,52 @@ class KrylovInfo:
     normres: float = float("nan")
 
 
-def _cgs2(V: List[np.ndarray], w: np.ndarray):
+class _KBasis:
+    """Krylov basis stored as the leading columns of one preallocated column-major
+    ``n x cap`` array (the projections are BLAS matrix-vector products on a view;
+    no copy of the basis per step)."""
+
+    def __init__(self, n: int, cap: int, v0: Optional[np.ndarray] = None):
+        self.B = np.empty((n, cap), dtype=C128, order="F")
+        self.m = 0
+        if v0 is not None:
+            self.append(v0)
+
+    def append(self, v):
+        self.B[:, self.m] = v
+        self.m += 1
+
+    def __len__(self):
+        return self.m
+
+    def __getitem__(self, k):
+        return self.B[:, k]
+
+    def mat(self, m: Optional[int] = None) -> np.ndarray:
+        return self.B[:, : (self.m if m is None else m)]
+
+    def reset(self, cols: np.ndarray):
+        """Replace the basis by the columns of ``cols`` (n x k)."""
+        k = cols.shape[1]
+        self.B[:, :k] = cols
+        self.m = k
+
+
+def _cgs2(V: "_KBasis", w: np.ndarray):
     """Classical Gram-Schmidt with iterative refinement (KrylovKit's
     ``ClassicalGramSchmidtIR`` with eta = 1/sqrt(2)): the projection is repeated
     while it shrank ||w|| below eta times its previous value, at most three passes."""
-    if not V:
+    if len(V) == 0:
         return w, np.zeros(0, dtype=C128)
-    B = np.stack(V, axis=1)
+    B = V.mat()
     nw0 = np.vdot(w, w).real
-    h = B.conj().T @ w
+    h = np.conj(np.conj(w) @ B)
     w = w - B @ h
     nw1 = np.vdot(w, w).real
     passes = 1
     while passes < 3 and nw1 < 0.5 * nw0:
         nw0 = nw1
-        h2 = B.conj().T @ w
+        h2 = np.conj(np.conj(w) @ B)
         w = w - B @ h2
         h = h + h2
         nw1 = np.vdot(w, w).real
@@ -393,7 +424,7 @@ def lanczos_eigsolve(A: Callable, x0: np.ndarray, tol: float, krylovdim: int = 3
     if beta0 == 0:
         raise ValueError("eigsolve: zero starting vector")
     x0n = x0f / beta0
-    V = [x0n.copy()]
+    V = _KBasis(n, kdim + 1, x0n)
     H = np.zeros((kdim + 1, kdim), dtype=C128)
     info = KrylovInfo(numiter=1)
     sign = 1.0 if which == "SR" else -1.0
@@ -418,22 +449,21 @@ def lanczos_eigsolve(A: Callable, x0: np.ndarray, tol: float, krylovdim: int = 3
             if res[0] <= tol or breakdown:
                 info.converged = 1
                 info.normres = float(res[0])
-                vec = np.stack(V, axis=1) @ U[:, 0]
+                vec = V.mat() @ U[:, 0]
                 vec /= np.linalg.norm(vec)
                 vec = _phase_align(vec, x0n)
                 return float(theta[0]), freshape(vec, shape), info
         if full:
             if info.numiter >= maxiter:
                 info.normres = float(res[0])
-                vec = np.stack(V, axis=1) @ U[:, 0]
+                vec = V.mat() @ U[:, 0]
                 vec /= np.linalg.norm(vec)
                 return float(theta[0]), freshape(vec, shape), info
             nconv = int(np.sum(res <= tol))
             keep = max(1, (3 * kdim + 2 * nconv) // 5)
-            B = np.stack(V, axis=1)
-            Vk = B @ U[:, :keep]
-            vnext = w / beta
-            V = [Vk[:, j].copy() for j in range(keep)] + [vnext]
+            Vk = V.mat() @ U[:, :keep]
+            V.reset(Vk)
+            V.append(w / beta)
             H = np.zeros((kdim + 1, kdim), dtype=C128)
             H[:keep, :keep] = np.diag(theta[:keep])
             H[keep, :keep] = beta * U[m - 1, :keep]
@@ -470,7 +500,7 @@ def gmres(A: Callable, b: np.ndarray, x0: np.ndarray, tol: float, krylovdim: int
     kdim = min(krylovdim, n)
     while True:
         info.numiter += 1
-        V = [r / beta]
+        V = _KBasis(n, kdim + 1, r / beta)
         R = np.zeros((kdim + 1, kdim), dtype=C128)
         cs = np.zeros(kdim, dtype=np.float64)
         sn = np.zeros(kdim, dtype=C128)
@@ -511,7 +541,7 @@ def gmres(A: Callable, b: np.ndarray, x0: np.ndarray, tol: float, krylovdim: int
         y = np.zeros(kused, dtype=C128)
         for i in range(kused - 1, -1, -1):
             y[i] = (g[i] - R[i, i + 1:kused] @ y[i + 1:kused]) / R[i, i]
-        x = x + np.stack(V[:kused], axis=1) @ y
+        x = x + V.mat(kused) @ y
         r = bf - op(x)
         beta = np.linalg.norm(r)
         info.normres = float(beta)
@@ -554,7 +584,7 @@ def exponentiate(A: Callable, t: complex, x: np.ndarray, tol: float = 1e-10,
             info.converged = 1
             return freshape(v, shape), info
         info.numiter += 1
-        V = [v / beta]
+        V = _KBasis(n, kdim + 1, v / beta)
         H = np.zeros((kdim + 1, kdim), dtype=C128)
         tau = remaining
         accepted = False
@@ -586,7 +616,7 @@ def exponentiate(A: Callable, t: complex, x: np.ndarray, tol: float = 1e-10,
         if accepted:
             m = len(V)
             E = _expm_herm(Hs, tau)
-            v = beta * (np.stack(V, axis=1) @ E[:, 0])
+            v = beta * (V.mat() @ E[:, 0])
             remaining = remaining - tau
             info.normres = float(err)
             if abs(remaining) <= 1e-15 * abs(T):
@@ -596,22 +626,58 @@ def exponentiate(A: Callable, t: complex, x: np.ndarray, tol: float = 1e-10,
                 return freshape(v, shape), info
 
 
+def _schur_sorted(M: np.ndarray):
+    """Complex Schur form ``M = Z T Z^H`` with ``|T[k,k]|`` non-increasing.
+
+    LAPACK's Schur form (scipy) reordered by adjacent swaps: the block
+    ``[[t11, t12], [0, t22]]`` has the eigenvector ``(t12, t22 - t11)`` for ``t22``,
+    and the unitary built from it moves ``t22`` up (LAPACK ``ztrexc``'s step)."""
+    import scipy.linalg as sl
+    T, Z = sl.schur(np.asarray(M, dtype=C128), output="complex")
+    T = np.array(T, dtype=C128)
+    Z = np.array(Z, dtype=C128)
+    n = T.shape[0]
+    for _ in range(n):
+        swapped = False
+        for k in range(n - 1):
+            t11, t22 = T[k, k], T[k + 1, k + 1]
+            if not abs(t22) > abs(t11):
+                continue
+            g = np.array([T[k, k + 1], t22 - t11])
+            nr = np.linalg.norm(g)
+            if nr == 0.0:
+                continue
+            g /= nr
+            G = np.array([[g[0], -np.conj(g[1])], [g[1], np.conj(g[0])]])
+            T[k:k + 2, :] = G.conj().T @ T[k:k + 2, :]
+            T[:, k:k + 2] = T[:, k:k + 2] @ G
+            Z[:, k:k + 2] = Z[:, k:k + 2] @ G
+            T[k + 1, k] = 0.0
+            T[k, k], T[k + 1, k + 1] = t22, t11
+            swapped = True
+        if not swapped:
+            break
+    return T, Z
+
+
 def arnoldi_dominant(A: Callable, x0: np.ndarray, tol: float, krylovdim: int = 30,
                      maxiter: int = 300, eager: bool = True):
     """Dominant (largest-magnitude) eigenpair of a non-Hermitian map.
 
     Restates ``gauge_fixedpoint`` (KrylovKit ``schursolve``, ``src/utility.jl:204-211``)
     and the ``:LM`` Arnoldi of ``dot(psi, psi)`` (``src/states/canonicalmps.jl:262-269``).
-    Arnoldi with CGS2; a Ritz pair is converged when ``|h_{m+1,m} y_m| <= tol``
-    (``y`` normalised).  A full basis restarts from the current dominant Ritz
-    vector.  The vector is normalised and phase-aligned with ``x0``.
+    Arnoldi with CGS2 in Krylov-Schur form ``A V_m = V_{m+1} H``; a Ritz pair ``(lam, V y)``
+    is converged when ``|H[m, :] y| <= tol`` (``y`` normalised).  A full basis restarts
+    from the leading ``keep = (3 krylovdim + 2 nconv) // 5`` Schur vectors of ``H[:m, :m]``
+    (sorted by ``|lambda|``) plus the residual vector, as ``schursolve`` does.  The vector
+    is normalised and phase-aligned with ``x0``.
     """
     shape = x0.shape
     x0f = np.asarray(x0, dtype=C128).ravel(order="F")
     n = x0f.size
     kdim = min(krylovdim, n)
     x0n = x0f / np.linalg.norm(x0f)
-    V = [x0n.copy()]
+    V = _KBasis(n, kdim + 1, x0n)
     H = np.zeros((kdim + 1, kdim), dtype=C128)
     info = KrylovInfo(numiter=1)
     while True:
@@ -626,24 +692,32 @@ def arnoldi_dominant(A: Callable, x0: np.ndarray, tol: float, krylovdim: int = 3
         lam, Y = np.linalg.eig(H[:m, :m])
         j = int(np.argmax(np.abs(lam)))
         y = Y[:, j] / np.linalg.norm(Y[:, j])
-        res = abs(hn * y[m - 1])
+        res = abs(H[m, :m] @ y)
         breakdown = hn <= 1e-14 * max(1.0, abs(lam[j]))
         full = m == kdim
         if eager or full or breakdown:
             if res <= tol or breakdown:
                 info.converged = 1
                 info.normres = float(res)
-                vec = np.stack(V, axis=1) @ y
+                vec = V.mat() @ y
                 vec /= np.linalg.norm(vec)
                 return complex(lam[j]), freshape(_phase_align(vec, x0n), shape), info
         if full:
-            vec = np.stack(V, axis=1) @ y
-            vec /= np.linalg.norm(vec)
             if info.numiter >= maxiter:
+                vec = V.mat() @ y
+                vec /= np.linalg.norm(vec)
                 info.normres = float(res)
                 return complex(lam[j]), freshape(vec, shape), info
-            V = [vec]
-            H = np.zeros((kdim + 1, kdim), dtype=C128)
+            T, Z = _schur_sorted(H[:m, :m])
+            nconv = 1 if res <= tol else 0
+            keep = max(1, min(m - 1, (3 * kdim + 2 * nconv) // 5))
+            Vm = V.mat() @ Z[:, :keep]
+            Hn = np.zeros((kdim + 1, kdim), dtype=C128)
+            Hn[:keep, :keep] = np.triu(T[:keep, :keep])
+            Hn[keep, :keep] = H[m, :m] @ Z[:, :keep]
+            V.reset(Vm)
+            V.append(w / hn)
+            H = Hn
             info.numiter += 1
         else:
             V.append(w / hn)
@@ -1277,26 +1351,8 @@ def find_groundstate(psi0: CanonicalIMPS, H: SchurMPO, alg: VUMPS, envs: Optiona
     losses = [eps]
     converged = False
     it = 0
-    N = len(psi)
     for it in range(1, alg.maxiter + 1):
-        siter = it - 1
-        ea = updatetol(alg.alg_eigsolve, siter, eps)
-        ALs = []
-        for site in range(N):
-            GL, W, GR = envs.lefts[site], H[site], envs.rights[site]
-            _, AC, _ = lanczos_eigsolve(lambda x: ac_apply(GL, W, GR, x), psi.AC[site], ea["tol"],
-                                        ea["krylovdim"], ea["maxiter"], ea["eager"])
-            GLc = envs.lefts[(site + 1) % N]
-            _, C, _ = lanczos_eigsolve(lambda x: c_apply(GLc, GR, x), psi.C[site], ea["tol"],
-                                       ea["krylovdim"], ea["maxiter"], ea["eager"])
-            ALs.append(regauge(AC, C))
-        ag = updatetol(alg.alg_gauge, siter, eps)
-        psi = canonical_from_AL_keepAL(ALs, psi.C[N - 1], ag["tol"], ag["maxiter"])
-        ae = updatetol(alg.alg_environments, siter, eps)
-        envs = build_envs(psi, H, tol=ae["tol"], maxiter=ae["maxiter"], init=envs)
-        if alg.finalize is not None:
-            psi, envs = alg.finalize(it, psi, H, envs)
-        eps = calc_galerkin(psi, H, envs)
+        psi, envs, eps = vumps_iteration(psi, H, envs, alg, it, eps)
         losses.append(eps)
         if log is not None:
             log.append(dict(iter=it, eps=eps, f=expectationvalue(psi, H, envs)))
@@ -1304,6 +1360,32 @@ def find_groundstate(psi0: CanonicalIMPS, H: SchurMPO, alg: VUMPS, envs: Optiona
             converged = True
             break
     return psi, envs, dict(niter=it, converged=converged, losses=losses, itererr=losses[-1])
+
+
+def vumps_iteration(psi: CanonicalIMPS, H: SchurMPO, envs: DMRGCache, alg: VUMPS, it: int, eps: float):
+    """One pass of the ``find_groundstate(::VUMPS)`` loop (``vumps.jl:51-85``) at outer
+    iteration ``it`` (1-based) after a Galerkin error ``eps``: ``localupdate_step!``
+    (``vumps.jl:7-19``), ``gauge_step!`` (``:23-31``), ``recalculate!`` and
+    ``calc_galerkin``.  Returns ``(psi, envs, eps_new)``."""
+    N = len(psi)
+    siter = it - 1
+    ea = updatetol(alg.alg_eigsolve, siter, eps)
+    ALs = []
+    for site in range(N):
+        GL, W, GR = envs.lefts[site], H[site], envs.rights[site]
+        _, AC, _ = lanczos_eigsolve(lambda x: ac_apply(GL, W, GR, x), psi.AC[site], ea["tol"],
+                                    ea["krylovdim"], ea["maxiter"], ea["eager"])
+        GLc = envs.lefts[(site + 1) % N]
+        _, C, _ = lanczos_eigsolve(lambda x: c_apply(GLc, GR, x), psi.C[site], ea["tol"],
+                                   ea["krylovdim"], ea["maxiter"], ea["eager"])
+        ALs.append(regauge(AC, C))
+    ag = updatetol(alg.alg_gauge, siter, eps)
+    psi = canonical_from_AL_keepAL(ALs, psi.C[N - 1], ag["tol"], ag["maxiter"])
+    ae = updatetol(alg.alg_environments, siter, eps)
+    envs = build_envs(psi, H, tol=ae["tol"], maxiter=ae["maxiter"], init=envs)
+    if alg.finalize is not None:
+        psi, envs = alg.finalize(it, psi, H, envs)
+    return psi, envs, calc_galerkin(psi, H, envs)
 
 
 def canonical_from_AL_keepAL(ALs, C0, tol, maxiter) -> CanonicalIMPS:
