@@ -2,8 +2,9 @@
 
 Usage: ``python -m infinitempsalgorithms_b200.build`` (or ``build()`` from Python).
 Compiles every ``csrc/*.cu`` into one shared library next to this file; the
-library links cuSOLVER (QRpos/LQpos) and the CUDA runtime and exports the C ABI
-declared in ``include/imps_b200.h``.
+library links only the CUDA runtime (every kernel, the QR factorisations
+included, is this package's own) and exports the C ABI declared in
+``include/imps_b200.h``.
 """
 from __future__ import annotations
 
@@ -51,7 +52,7 @@ def build(verbose: bool = False, extra=()) -> Path:
         objs = list(ex.map(lambda s: _compile(s, list(extra)), srcs))
     newest = max(o.stat().st_mtime for o in objs)
     if not LIB.exists() or LIB.stat().st_mtime < newest:
-        cmd = [nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lcusolver", "-lcudart"]
+        cmd = [nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lcudart"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

@@ -121,8 +121,6 @@ int imps_ctx_create(int device, imps_ctx** out) {
     IMPS_CUDA(cudaSetDevice(device));
     IMPS_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
     c.own_stream = true;
-    IMPS_SOLVER(cusolverDnCreate(&c.solver));
-    IMPS_SOLVER(cusolverDnSetStream(c.solver, c.stream));
     IMPS_CUDA(cudaMalloc((void**)&c.dev_info, sizeof(int) * 4));
     IMPS_CUDA(cudaMalloc((void**)&c.err_dev, sizeof(int) * 4));
     IMPS_CUDA(cudaMemset(c.err_dev, 0, sizeof(int) * 4));
@@ -159,7 +157,6 @@ int imps_ctx_destroy(imps_ctx* h) {
   if (c.dev_info) cudaFree(c.dev_info);
   if (c.err_dev) cudaFree(c.err_dev);
   if (c.err_host) cudaFreeHost(c.err_host);
-  if (c.solver) cusolverDnDestroy(c.solver);
   if (c.own_stream && c.stream) cudaStreamDestroy(c.stream);
   delete h;
   return IMPS_OK;
@@ -173,7 +170,6 @@ int imps_ctx_set_stream(imps_ctx* h, void* stream) {
     if (c.own_stream && c.stream) cudaStreamDestroy(c.stream);
     c.stream = static_cast<cudaStream_t>(stream);
     c.own_stream = false;
-    IMPS_SOLVER(cusolverDnSetStream(c.solver, c.stream));
     return IMPS_OK;
   });
 }

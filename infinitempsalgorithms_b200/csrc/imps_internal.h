@@ -6,7 +6,6 @@
 #pragma once
 
 #include <cuda_runtime.h>
-#include <cusolverDn.h>
 
 #include <complex>
 #include <cstdint>
@@ -42,15 +41,6 @@ struct Error : public std::runtime_error {
                                                " at " + __FILE__ + ":" +              \
                                                std::to_string(__LINE__));             \
     }                                                                                 \
-  } while (0)
-
-#define IMPS_SOLVER(call)                                                                 \
-  do {                                                                                    \
-    cusolverStatus_t s_ = (call);                                                         \
-    if (s_ != CUSOLVER_STATUS_SUCCESS)                                                    \
-      throw ::imps::Error(IMPS_CUDA_ERROR, std::string("cusolver status ") +             \
-                                               std::to_string((int)s_) + " at " +         \
-                                               __FILE__ + ":" + std::to_string(__LINE__)); \
   } while (0)
 
 #define IMPS_REQUIRE(cond, status, msg)        \
@@ -105,7 +95,6 @@ struct Context {
   int device = 0;
   cudaStream_t stream = nullptr;
   bool own_stream = true;
-  cusolverDnHandle_t solver = nullptr;
   int precision = PREC_FP64;
   int nslices = 5;           // int8 slices per operand in split mode
   bool adaptive_slices = false;
