@@ -55,6 +55,8 @@ __all__ = [
     "state_dot", "DMRGCache", "build_envs", "ac_apply", "c_apply", "calc_galerkin",
     "expectationvalue", "local_expectation1", "VUMPS", "TDVP", "IDMRG",
     "find_groundstate", "vumps_iteration", "timestep", "time_evolve", "idmrg_groundstate",
+    "dominant_env", "normalize_envs", "build_envs_dense", "expectationvalue_dense", "apply_local", "correlator",
+    "entanglement_spectrum", "renyi_entropy", "entropy",
 ]
 
 C128 = np.complex128
@@ -1486,3 +1488,137 @@ def idmrg_groundstate(psi0: CanonicalIMPS, H: SchurMPO, alg: IDMRG, envs: Option
     psi2 = canonical_from_sites([psi.AR[l] for l in range(N)], tol=ag["tol"], maxiter=ag["maxiter"])
     envs2 = build_envs(psi2, H, init=envs)
     return psi2, envs2, dict(niter=it, converged=converged, losses=losses, itererr=losses[-1], E=E)
+
+
+# --------------------------------------------------------------------------
+# Dense-MPO channel, correlators and entanglement (src/algorithms/groundstates/envs.jl:34-99,
+# 284-304, 559-584; src/observables/expval.jl:60-79; src/observables/correlators.jl:13-42;
+# src/observables/toolbox.jl:9-25)
+# --------------------------------------------------------------------------
+def dominant_env(psi: CanonicalIMPS, W: Optional[Sequence[np.ndarray]] = None, side: str = "left",
+                 tol: float = Defaults.tol, krylovdim: int = Defaults.krylovdim, maxiter: int = Defaults.maxiter):
+    """``dominant_env([W,] psi; side)`` (``envs.jl:34-99``): dominant (``:LM``) eigenvector of
+    the identity (``W is None``, ``AL``/``AR`` pushes) or dense-MPO transfer matrix of one unit
+    cell, from ``v0 = ones``, returned as ``(lambda, L)`` with ``L`` of shape
+    ``(D, w, D)`` (``w = 1`` for the identity channel) and unit Frobenius norm."""
+    N = len(psi)
+    D = psi.AL[0].shape[0]
+    w = 1 if W is None else W[0].shape[0]
+
+    def tm(v):
+        L = v
+        if W is None:
+            if side == "left":
+                for l in range(N):
+                    L = push_env_left(L, psi.AL[l])
+            else:
+                for l in range(N - 1, -1, -1):
+                    L = push_env_right(L, psi.AR[l])
+            return L
+        if side == "left":
+            for l in range(N):
+                L = push_mpo_left(L, W[l], psi.AL[l])
+        else:
+            for l in range(N - 1, -1, -1):
+                L = push_mpo_right(L, W[l], psi.AR[l])
+        return L
+    shape = (D, D) if W is None else (D, w, D)
+    v0 = np.ones(shape, dtype=C128, order="F")
+    lam, vec, _ = arnoldi_dominant(tm, v0, tol, krylovdim, maxiter, eager=True)
+    L = freshape(np.asarray(vec), (D, w, D))
+    return lam, np.asfortranarray(L / np.linalg.norm(L))
+
+
+def normalize_envs(envs: "DMRGCache", psi: CanonicalIMPS) -> "DMRGCache":
+    """``normalize_envs!(envs, below, operator, above)`` (``envs.jl:559-584``): every right
+    environment to unit norm, then ``lefts[i+1] /= <C_i, H_C(i) C_i>``."""
+    N = len(psi)
+    for i in range(N):
+        nr = np.linalg.norm(envs.rights[i])
+        if nr > 0:
+            envs.rights[i] = envs.rights[i] / nr
+        lam = np.vdot(psi.C[i], c_apply(envs.lefts[(i + 1) % N], envs.rights[i], psi.C[i]))
+        if abs(lam) > 0:
+            envs.lefts[(i + 1) % N] = envs.lefts[(i + 1) % N] / lam
+    return envs
+
+
+def build_envs_dense(psi: CanonicalIMPS, W: Sequence[np.ndarray], tol: float = Defaults.tol,
+                     krylovdim: int = Defaults.krylovdim, maxiter: int = Defaults.maxiter) -> "DMRGCache":
+    """``DMRGCache(psi, ::DenseIMPO)`` (``envs.jl:284-304``): dominant left / right environments
+    of the dense-MPO transfer matrix, pushed around the unit cell, then ``normalize_envs``."""
+    N = len(psi)
+    _, L0 = dominant_env(psi, W, "left", tol, krylovdim, maxiter)
+    _, R0 = dominant_env(psi, W, "right", tol, krylovdim, maxiter)
+    lefts = [None] * N
+    rights = [None] * N
+    lefts[0] = L0
+    for l in range(1, N):
+        lefts[l] = push_mpo_left(lefts[l - 1], W[l - 1], psi.AL[l - 1])
+    rights[N - 1] = R0
+    for l in range(N - 2, -1, -1):
+        rights[l] = push_mpo_right(rights[l + 1], W[l + 1], psi.AR[l + 1])
+    return normalize_envs(DMRGCache(lefts, rights), psi)
+
+
+def expectationvalue_dense(psi: CanonicalIMPS, W: Sequence[np.ndarray], envs: "DMRGCache") -> complex:
+    """``expectationvalue(psi, ::DenseIMPO, envs)`` (``expval.jl:60-79``): the sum over the unit
+    cell of ``contract_mpo_expval(AC_i, GL_i, W_i, GR_i) = <AC_i, H_AC(i) AC_i>``, divided by
+    ``<psi|psi>``."""
+    N = len(psi)
+    E = 0j
+    for i in range(N):
+        E += np.vdot(psi.AC[i], ac_apply(envs.lefts[i], W[i], envs.rights[i], psi.AC[i]))
+    return E / state_dot(psi, psi)
+
+
+def apply_local(O: np.ndarray, A: np.ndarray) -> np.ndarray:
+    """``A'[a, u, b] = sum_s O[u, s] A[a, s, b]``."""
+    return np.asfortranarray(np.einsum("us,asb->aub", O, A))
+
+
+def correlator(psi: CanonicalIMPS, O1: np.ndarray, O2: np.ndarray, i: int, js: Sequence[int]) -> np.ndarray:
+    """``correlator(psi, O1, O2, i, js)`` (``correlators.jl:13-42``): ``<O1_i O2_j> / <psi|psi>``
+    for every ``j`` in ``js`` (1-based sites, increasing, ``j > i``).  As in the reference,
+    the identity transfer through ``AR`` runs over sites ``ctr+1 .. j-1`` with ``ctr`` the
+    previously evaluated ``j`` (the reference sets ``ctr = j`` after each value)."""
+    N = len(psi)
+    js = list(js)
+    if js[0] <= i:
+        raise ValueError("i should be smaller than j")
+    AC = psi.AC[(i - 1) % N]
+    V = push_env_left(np.eye(AC.shape[0], dtype=C128), apply_local(O1, AC), AC)
+    out = np.zeros(len(js), dtype=C128)
+    ctr = i
+    for k, j in enumerate(js):
+        for l in range(ctr + 1, j):
+            A = psi.AR[(l - 1) % N]
+            V = push_env_left(V, A, A)
+        AR = psi.AR[(j - 1) % N]
+        E = push_env_left(V, apply_local(O2, AR), AR)
+        out[k] = np.trace(E)
+        ctr = j
+    return out / state_dot(psi, psi)
+
+
+def entanglement_spectrum(psi: CanonicalIMPS, loc: int = 1) -> np.ndarray:
+    """``entanglement_spectrum(psi, loc)`` (``toolbox.jl:9-14``): squared singular values of
+    ``C[loc]`` (1-based bond, periodic), normalised, descending."""
+    N = len(psi)
+    s = np.linalg.svd(psi.C[(loc - 1) % N], compute_uv=False)
+    p = np.abs(s) ** 2
+    return np.sort(p / p.sum())[::-1]
+
+
+def renyi_entropy(p: np.ndarray, alpha: float = 1.0) -> float:
+    """von Neumann (``alpha = 1``) or Renyi entropy of a probability vector (natural log)."""
+    p = np.asarray(p, dtype=float)
+    p = p[p > 0]
+    if alpha == 1:
+        return float(-np.sum(p * np.log(p)))
+    return float(np.log(np.sum(p ** alpha)) / (1.0 - alpha))
+
+
+def entropy(psi: CanonicalIMPS, loc: int = 1, alpha: float = 1.0) -> float:
+    """``entropy(psi, loc; alpha)`` (``toolbox.jl:16-25``)."""
+    return renyi_entropy(entanglement_spectrum(psi, loc), alpha)
