@@ -269,6 +269,31 @@ int imps_energy(imps_envs* envs, const imps_mpo* mpo, imps_state* st, double* re
 /* expectationvalue(psi, (site,) => O) (src/observables/expval.jl:33-37); O is d x d. */
 int imps_local_expval(imps_state* st, int site, const double* O, double* re, double* im);
 
+/* ------------------------------------- dense-MPO channel and observables */
+/* dominant_env([W,] psi; side) (src/algorithms/groundstates/envs.jl:34-99): dominant
+ * (:LM) eigenvector of the transfer matrix of one unit cell, identity channel (AL / AR
+ * pushes) when mpo is NULL, else the dense-MPO channel of `mpo` (the tompotensors taken
+ * as a DenseIMPO); side 0 = left, 1 = right.  Arnoldi from v0 = ones; L_host receives
+ * the unit-norm (D, w, D) environment (w = 1 for the identity channel), lambda[0..1]
+ * the eigenvalue. */
+int imps_dominant_env(imps_state* st, const imps_mpo* mpo, int side, double tol, int krylovdim, int maxiter,
+                      double* lambda, double* L_host, imps_krylov_info* info);
+/* DMRGCache(psi, ::DenseIMPO) (envs.jl:284-304): dominant left / right environments
+ * pushed around the unit cell, then normalize_envs! (envs.jl:559-584). */
+int imps_envs_build_dense(imps_envs* envs, imps_state* st, const imps_mpo* mpo, double tol, int krylovdim,
+                          int maxiter, imps_krylov_info* info);
+/* expectationvalue(psi, ::DenseIMPO, envs) (src/observables/expval.jl:60-79). */
+int imps_energy_dense(imps_envs* envs, const imps_mpo* mpo, imps_state* st, double* re, double* im);
+/* correlator(psi, O1, O2, i, js) (src/observables/correlators.jl:13-42): <O1_i O2_j> /
+ * <psi|psi> for the nj increasing 1-based sites js (> i); O1, O2 are d x d column-major
+ * complex; out receives nj interleaved complex values.  As in the reference, a later j
+ * transfers through AR from the previous j + 1 on. */
+int imps_correlator(imps_state* st, const double* O1, const double* O2, int i, int nj, const int* js, double* out);
+/* entanglement_spectrum(psi, loc) (src/observables/toolbox.jl:9-14) of bond `bond`
+ * (0-based, bond l right of site l): the chi normalised squared singular values of C,
+ * descending (one-sided Jacobi on the device); p holds chi doubles. */
+int imps_entanglement_spectrum(imps_state* st, int bond, double* p);
+
 /* ---------------------------------------------------------------- gradients */
 /* No counterpart in the reference (an extension for gradient-based iMPS
  * optimisation).  Both use the environments in `envs`, which must be the fixed

@@ -80,6 +80,11 @@ _SIGS = {
     "imps_ctx_set_precision": (I32, [P, I32, I32]),
     "imps_ctx_synchronize": (I32, [P]),
     "imps_ctx_set_wait_limit": (I32, [P, I64]),
+    "imps_dominant_env": (I32, [P, P, I32, D, I32, I32, DP, DP, C.POINTER(KrylovInfo)]),
+    "imps_envs_build_dense": (I32, [P, P, P, D, I32, I32, C.POINTER(KrylovInfo)]),
+    "imps_energy_dense": (I32, [P, P, P, DP, DP]),
+    "imps_correlator": (I32, [P, DP, DP, I32, I32, C.POINTER(I32), DP]),
+    "imps_entanglement_spectrum": (I32, [P, I32, DP]),
     "imps_ctx_set_workspace_limit": (I32, [P, I64]),
     "imps_ctx_workspace_bytes": (I32, [P, C.POINTER(I64)]),
     "imps_ctx_counters_ext": (I32, [P, C.POINTER(I64), I32]),

@@ -29,6 +29,7 @@ __all__ = [
     "IDMRG", "TDVP", "IterativeConvergenceInfo", "find_groundstate", "timestep", "time_evolve", "linsolve",
     "qrpos", "lqpos", "push_env_left", "push_env_right", "push_mpo_left", "push_mpo_right",
     "energy_gradient_mpo", "energy_gradient_AL", "coupling_gradient", "rrule_energy", "find_groundstate_batch",
+    "DenseIMPO", "identityimpo", "dominant_env", "correlator", "entanglement_spectrum", "renyi_entropy", "entropy",
 ]
 
 
@@ -264,6 +265,19 @@ class SparseIMPO:
                 pass
 
 
+class DenseIMPO(SparseIMPO):
+    """``DenseIMPO``: a periodic string of dense MPO tensors ``(m, d, n, d)`` without the
+    Schur structure (transfer matrices, time-evolution MPOs).  Its environments are
+    the dominant fixed points of the MPO transfer matrix (``DMRGCache(psi, ::DenseIMPO)``,
+    ``src/algorithms/groundstates/envs.jl:284-304``) and its expectation value is the
+    sum of the local contractions (``src/observables/expval.jl:60-79``)."""
+
+
+def identityimpo(dims: Sequence[int]) -> DenseIMPO:
+    """The identity MPO (bond dimension 1) on a unit cell with physical dimensions ``dims``."""
+    return DenseIMPO([np.eye(d, dtype=complex).reshape(1, d, 1, d) for d in dims])
+
+
 class _MpoHandle:
     """Weak link from a context to an MPO's device copy on it (released with the context)."""
 
@@ -487,6 +501,12 @@ class DMRGCache:
             self.build(psi, H, tol=tol, maxiter=maxiter, krylovdim=krylovdim, warm=False)
 
     def build(self, psi, H, tol=Defaults.tol, maxiter=Defaults.maxiter, krylovdim=Defaults.krylovdim, warm=True):
+        if isinstance(H, DenseIMPO):
+            kinfo = L.KrylovInfo()
+            check(self.ctx.lib.imps_envs_build_dense(self.h, psi.h, H.handle(self.ctx), tol, krylovdim, maxiter,
+                                                     C.byref(kinfo)), self.ctx.h)
+            self.info = kinfo
+            return self
         info = L.EnvInfo()
         check(self.ctx.lib.imps_envs_build(self.h, psi.h, H.handle(self.ctx), tol, maxiter, krylovdim, int(warm),
                                            C.byref(info)), self.ctx.h)
@@ -732,6 +752,11 @@ def expectationvalue(psi: CanonicalIMPS, O=None, envs: Optional[DMRGCache] = Non
     ctx = psi.ctx
     if O is None:
         return psi.dot()
+    if isinstance(O, DenseIMPO):
+        envs = envs or DMRGCache(psi, O)
+        re, im = C.c_double(), C.c_double()
+        check(ctx.lib.imps_energy_dense(envs.h, O.handle(ctx), psi.h, C.byref(re), C.byref(im)), ctx.h)
+        return complex(re.value, im.value)
     if isinstance(O, SparseIMPO):
         envs = envs or DMRGCache(psi, O)
         re, im = C.c_double(), C.c_double()
@@ -747,6 +772,58 @@ def expectationvalue(psi: CanonicalIMPS, O=None, envs: Optional[DMRGCache] = Non
         check(ctx.lib.imps_local_expval(psi.h, (sites[0] - 1) % psi.N, dptr(op), C.byref(re), C.byref(im)), ctx.h)
         return complex(re.value, im.value)
     raise TypeError("unsupported operator")
+
+
+def dominant_env(psi: CanonicalIMPS, W: Optional[DenseIMPO] = None, side: str = "left", tol=Defaults.tol,
+                 krylovdim=Defaults.krylovdim, maxiter=Defaults.maxiter):
+    """``dominant_env([W,] psi; side)`` (``envs.jl:34-99``) -> ``(lambda, L)`` with ``L`` of
+    shape ``(D, w, D)`` (``w = 1`` without an MPO), unit norm."""
+    ctx = psi.ctx
+    D = psi.chi[-1]
+    w = 1 if W is None else W[1].shape[0]
+    L_ = np.zeros((D, w, D), complex, order="F")
+    lam = np.zeros(2)
+    info = L.KrylovInfo()
+    check(ctx.lib.imps_dominant_env(psi.h, None if W is None else W.handle(ctx), 0 if side == "left" else 1, tol,
+                                    krylovdim, maxiter, lam.ctypes.data_as(L.DP), dptr(L_), C.byref(info)), ctx.h)
+    return complex(lam[0], lam[1]), L_
+
+
+def correlator(psi: CanonicalIMPS, O1: np.ndarray, O2: np.ndarray, i: int, js) -> np.ndarray:
+    """``correlator(psi, O1, O2, i, js)`` (``correlators.jl:13-42``): ``<O1_i O2_j>/<psi|psi>``
+    for an int ``js`` (a number) or an increasing range of 1-based sites ``j > i``."""
+    single = isinstance(js, (int, np.integer))
+    jl = [int(js)] if single else [int(j) for j in js]
+    if not jl or jl[0] <= i:
+        raise L.ArgumentError(L.IMPS_INVALID_ARG, f"i should be smaller than j ({i}, {jl[0] if jl else None})")
+    ctx = psi.ctx
+    arr = (C.c_int * len(jl))(*jl)
+    out = np.zeros(len(jl), complex)
+    check(ctx.lib.imps_correlator(psi.h, dptr(cbuf(O1)), dptr(cbuf(O2)), int(i), len(jl), arr, dptr(out)), ctx.h)
+    return out[0] if single else out
+
+
+def entanglement_spectrum(psi: CanonicalIMPS, loc: int = 1) -> np.ndarray:
+    """``entanglement_spectrum(psi, loc)`` (``toolbox.jl:9-14``): normalised squared Schmidt
+    values of bond ``loc`` (1-based, right of site ``loc``), descending."""
+    b = (loc - 1) % psi.N
+    p = np.zeros(psi.chi[b])
+    check(psi.ctx.lib.imps_entanglement_spectrum(psi.h, b, p.ctypes.data_as(L.DP)), psi.ctx.h)
+    return p
+
+
+def renyi_entropy(p, alpha: float = 1.0) -> float:
+    """von Neumann (``alpha = 1``) or Renyi entropy of a probability vector (natural log)."""
+    p = np.asarray(p, dtype=float)
+    p = p[p > 0]
+    if alpha == 1:
+        return float(-np.sum(p * np.log(p)))
+    return float(np.log(np.sum(p ** alpha)) / (1.0 - alpha))
+
+
+def entropy(psi: CanonicalIMPS, loc: int = 1, alpha: float = 1.0) -> float:
+    """``entropy(psi, loc; alpha)`` (``toolbox.jl:16-25``)."""
+    return renyi_entropy(entanglement_spectrum(psi, loc), alpha)
 
 
 # ---------------------------------------------------------------------------

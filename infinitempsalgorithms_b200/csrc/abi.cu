@@ -15,6 +15,7 @@
 #include "imps_internal.h"
 #include "krylov.h"
 #include "mpo.h"
+#include "observables.h"
 
 struct imps_ctx {
   imps::Context c;
@@ -889,6 +890,68 @@ int imps_local_expval(imps_state* st, int site, const double* O, double* re, dou
     imps::cplx v = imps::local_expval(st->ctx, st, site, hc(O));
     if (re) *re = v.real();
     if (im) *im = v.imag();
+    return IMPS_OK;
+  });
+}
+
+// -------------------------------------------- dense-MPO channel and observables
+int imps_dominant_env(imps_state* st, const imps_mpo* mpo, int side, double tol, int krylovdim, int maxiter,
+                      double* lambda, double* L_host, imps_krylov_info* info) {
+  if (!st || (side != 0 && side != 1)) return IMPS_INVALID_ARG;
+  return guard(st->ctx, [&] {
+    imps::Context* ctx = st->ctx;
+    const int D = st->Dl(0), w = mpo ? mpo->sites[0].m : 1;
+    const size_t n = (size_t)D * w * D;
+    imps::DevBuf& out = ctx->buf("abi_domenv", n * sizeof(imps::dcplx));
+    imps::KrylovResult r = imps::dominant_env(ctx, st, mpo, side, tol, krylovdim, maxiter, out.z());
+    if (lambda) {
+      lambda[0] = r.value.real();
+      lambda[1] = r.value.imag();
+    }
+    if (L_host) imps::download(ctx, L_host, out.ptr, n * sizeof(imps::dcplx));
+    fill_info(info, r);
+    return conv_status(r.converged);
+  });
+}
+
+int imps_envs_build_dense(imps_envs* E, imps_state* st, const imps_mpo* mpo, double tol, int krylovdim,
+                          int maxiter, imps_krylov_info* info) {
+  if (!E || !st || !mpo) return IMPS_INVALID_ARG;
+  return guard(E->ctx, [&] {
+    imps::KrylovResult r = imps::envs_build_dense(E->ctx, E, st, mpo, tol, krylovdim, maxiter);
+    fill_info(info, r);
+    return conv_status(r.converged);
+  });
+}
+
+int imps_energy_dense(imps_envs* E, const imps_mpo* mpo, imps_state* st, double* re, double* im) {
+  if (!E || !mpo || !st) return IMPS_INVALID_ARG;
+  return guard(E->ctx, [&] {
+    imps::cplx e = imps::energy_dense(E->ctx, E, mpo, st);
+    if (re) *re = e.real();
+    if (im) *im = e.imag();
+    return IMPS_OK;
+  });
+}
+
+int imps_correlator(imps_state* st, const double* O1, const double* O2, int i, int nj, const int* js, double* out) {
+  if (!st || !O1 || !O2 || !js || !out || nj <= 0) return IMPS_INVALID_ARG;
+  return guard(st->ctx, [&] {
+    std::vector<int> jv(js, js + nj);
+    std::vector<imps::cplx> g = imps::correlator(st->ctx, st, hc(O1), hc(O2), i, jv);
+    for (int k = 0; k < nj; ++k) {
+      out[2 * k] = g[k].real();
+      out[2 * k + 1] = g[k].imag();
+    }
+    return IMPS_OK;
+  });
+}
+
+int imps_entanglement_spectrum(imps_state* st, int bond, double* p) {
+  if (!st || !p) return IMPS_INVALID_ARG;
+  return guard(st->ctx, [&] {
+    std::vector<double> v = imps::entanglement_spectrum(st->ctx, st, bond);
+    std::copy(v.begin(), v.end(), p);
     return IMPS_OK;
   });
 }
