@@ -350,6 +350,9 @@ def run_ours(args, world, rank, local):
         c64.set_stream(stream.cuda_stream)
         psi64 = imps.CanonicalIMPS(c64, [4] * N, [D] * N)
         envs64 = imps.DMRGCache(psi64, H, build=False)
+        # one untimed FP64 iteration first (buffers of the FP64 context, its kernels)
+        restore(c64, psi64, envs64, snap0)
+        timed_iterations(c64, H, psi64, envs64, eps0, 1, stream)
         restore(c64, psi64, envs64, snap0)
         ms64, per64, inf64, _ = timed_iterations(c64, H, psi64, envs64, eps0, k64, stream)
         ms_s = sum(per_ms[:k64])

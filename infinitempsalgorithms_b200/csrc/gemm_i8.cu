@@ -102,15 +102,24 @@ __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 // bounded wait: returns false (and raises the error flag) after `limit` cycles.  The
-// fast path only polls the barrier; the global error flag and the clock are checked
-// every 256 unsuccessful polls so a completed phase is seen without extra memory
-// latency.
+// fast path only polls the barrier; the clock is also read on the first unsuccessful
+// poll (so a bound shorter than a poll round trips at once) and the global error
+// flag with the clock every 256 unsuccessful polls, so a completed phase is seen
+// without extra memory latency.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* err, long long limit) {
   if (mbar_try(bar, parity)) return true;
   const long long t0 = clock64();
   unsigned spins = 0;
   while (!mbar_try(bar, parity)) {
-    if ((++spins & 255u) != 0u) continue;
+    ++spins;
+    if (spins == 1u) {
+      if (clock64() - t0 > limit) {
+        atomicExch((int*)err, 1);
+        return false;
+      }
+      continue;
+    }
+    if ((spins & 255u) != 0u) continue;
     if (*err) return false;
     if (clock64() - t0 > limit) {
       atomicExch((int*)err, 1);
