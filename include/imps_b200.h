@@ -294,6 +294,15 @@ int imps_correlator(imps_state* st, const double* O1, const double* O2, int i, i
  * descending (one-sided Jacobi on the device); p holds chi doubles. */
 int imps_entanglement_spectrum(imps_state* st, int bond, double* p);
 
+/* timeevompo(H::SparseIMPO, delta, WI()/WII()) (src/algorithms/timeevo/w1w2.jl:26-45),
+ * one site: from the Schur tensor W (m, d, n, d) (level 1 and level m = n the identity
+ * levels) the W^I (alg = 1) or W^II (alg = 2) tensor (m-1, d, n-1, d) of the dense
+ * MPO approximating exp(delta H), by the block-exponential construction of
+ * arXiv:1407.1832 (the reference's own kernel is in an unvendored package).  Host
+ * computation, needs no device; out is caller-owned. */
+int imps_timeevompo_tensor(int m, int d, int n, const double* W, double delta_re, double delta_im, int alg,
+                           double* out);
+
 /* ---------------------------------------------------------------- gradients */
 /* No counterpart in the reference (an extension for gradient-based iMPS
  * optimisation).  Both use the environments in `envs`, which must be the fixed

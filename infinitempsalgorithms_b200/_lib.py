@@ -80,6 +80,7 @@ _SIGS = {
     "imps_ctx_set_precision": (I32, [P, I32, I32]),
     "imps_ctx_synchronize": (I32, [P]),
     "imps_ctx_set_wait_limit": (I32, [P, I64]),
+    "imps_timeevompo_tensor": (I32, [I32, I32, I32, DP, D, D, I32, DP]),
     "imps_dominant_env": (I32, [P, P, I32, D, I32, I32, DP, DP, C.POINTER(KrylovInfo)]),
     "imps_envs_build_dense": (I32, [P, P, P, D, I32, I32, C.POINTER(KrylovInfo)]),
     "imps_energy_dense": (I32, [P, P, P, DP, DP]),

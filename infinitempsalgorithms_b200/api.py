@@ -29,7 +29,7 @@ __all__ = [
     "IDMRG", "TDVP", "IterativeConvergenceInfo", "find_groundstate", "timestep", "time_evolve", "linsolve",
     "qrpos", "lqpos", "push_env_left", "push_env_right", "push_mpo_left", "push_mpo_right",
     "energy_gradient_mpo", "energy_gradient_AL", "coupling_gradient", "rrule_energy", "find_groundstate_batch",
-    "DenseIMPO", "identityimpo", "dominant_env", "correlator", "entanglement_spectrum", "renyi_entropy", "entropy",
+    "DenseIMPO", "identityimpo", "timeevompo", "dominant_env", "correlator", "entanglement_spectrum", "renyi_entropy", "entropy",
 ]
 
 
@@ -772,6 +772,24 @@ def expectationvalue(psi: CanonicalIMPS, O=None, envs: Optional[DMRGCache] = Non
         check(ctx.lib.imps_local_expval(psi.h, (sites[0] - 1) % psi.N, dptr(op), C.byref(re), C.byref(im)), ctx.h)
         return complex(re.value, im.value)
     raise TypeError("unsupported operator")
+
+
+def timeevompo(H: SparseIMPO, delta: complex, alg: str = "WII") -> DenseIMPO:
+    """``timeevompo(H::SparseIMPO, delta, WI()/WII())`` (``w1w2.jl:26-31``): the dense MPO
+    approximating ``exp(delta H)`` (real time: ``delta = -i dt``; imaginary: ``-tau``), one
+    W^I / W^II tensor per site of the unit cell."""
+    code = {"WI": 1, "WII": 2}.get(alg)
+    if code is None:
+        raise L.ArgumentError(L.IMPS_INVALID_ARG, "alg must be 'WI' or 'WII'")
+    lib = L.load()
+    delta = complex(delta)
+    out = []
+    for W in H.Ws:
+        m, d, n = W.shape[0], W.shape[1], W.shape[2]
+        o = np.zeros((m - 1, d, n - 1, d), complex, order="F")
+        check(lib.imps_timeevompo_tensor(m, d, n, dptr(cbuf(W)), delta.real, delta.imag, code, dptr(o)))
+        out.append(o)
+    return DenseIMPO(out)
 
 
 def dominant_env(psi: CanonicalIMPS, W: Optional[DenseIMPO] = None, side: str = "left", tol=Defaults.tol,

@@ -956,6 +956,15 @@ int imps_entanglement_spectrum(imps_state* st, int bond, double* p) {
   });
 }
 
+int imps_timeevompo_tensor(int m, int d, int n, const double* W, double delta_re, double delta_im, int alg,
+                           double* out) {
+  if (!W || !out) return IMPS_INVALID_ARG;
+  return guard(nullptr, [&] {
+    imps::timeevompo_site(m, d, n, hc(W), imps::cplx(delta_re, delta_im), alg, reinterpret_cast<imps::cplx*>(out));
+    return IMPS_OK;
+  });
+}
+
 // ------------------------------------------------------------------ gradients
 int imps_energy_grad_mpo(imps_envs* E, const imps_mpo* mpo, imps_state* st, int site, double* G) {
   if (!E || !mpo || !st || !G) return IMPS_INVALID_ARG;

@@ -378,6 +378,9 @@ void ac_apply_noalloc(Context* ctx, int Dl, int d, int Dr, int m, int n, const c
 size_t noalloc_scratch_bytes();
 // Loads the no-alloc array on `device` (current) and caches its address.
 void noalloc_prepare(int device);
+// W^I (alg 1) / W^II (alg 2) tensor (m-1, d, n-1, d) of the Schur site tensor W (m, d, n, d)
+// approximating exp(delta H) (timeevo_mpo.cu; host only).
+void timeevompo_site(int m, int d, int n, const cplx* W, cplx delta, int alg, cplx* out);
 // Full MPO pushes (transfer_leftenv!/transfer_rightenv!)
 void push_mpo_left(Context* ctx, const MpoSite& W, int Dl, int d, int Dr, const dcplx* L, const dcplx* A, dcplx* out);
 void push_mpo_right(Context* ctx, const MpoSite& W, int Dl, int d, int Dr, const dcplx* R, const dcplx* A,

@@ -57,6 +57,7 @@ __all__ = [
     "find_groundstate", "vumps_iteration", "timestep", "time_evolve", "idmrg_groundstate",
     "dominant_env", "normalize_envs", "build_envs_dense", "expectationvalue_dense", "apply_local", "correlator",
     "entanglement_spectrum", "renyi_entropy", "entropy",
+    "timeevompo", "timeevompo_site", "mpo_ring",
 ]
 
 C128 = np.complex128
@@ -1622,3 +1623,91 @@ def renyi_entropy(p: np.ndarray, alpha: float = 1.0) -> float:
 def entropy(psi: CanonicalIMPS, loc: int = 1, alpha: float = 1.0) -> float:
     """``entropy(psi, loc; alpha)`` (``toolbox.jl:16-25``)."""
     return renyi_entropy(entanglement_spectrum(psi, loc), alpha)
+
+
+# --------------------------------------------------------------------------
+# Time-evolution MPOs W^I / W^II (src/algorithms/timeevo/w1w2.jl:26-45).  The per-site
+# kernel lives in the unvendored FiniteMPSAlgorithms package; this restates the
+# published construction (Zaletel, Mong, Karrasch, Moore, Pollmann, PRB 91, 165112
+# (2015), arXiv:1407.1832), which the reference cites.  Parity unpinned: only the
+# physics (exp(delta H) to first order, the W^II error O(delta^2)) pins it.
+# --------------------------------------------------------------------------
+def _schur_blocks(W: np.ndarray):
+    """Schur pieces of one site tensor W (m, d, n, d): D = W[0,:,n-1,:], C_b = W[0,:,b,:]
+    (b interior), B_a = W[a,:,n-1,:], A_ab = W[a,:,b,:]."""
+    m, n = W.shape[0], W.shape[2]
+    D = W[0, :, n - 1, :]
+    C = [W[0, :, b, :] for b in range(1, n - 1)]
+    B = [W[a, :, n - 1, :] for a in range(1, m - 1)]
+    A = [[W[a, :, b, :] for b in range(1, n - 1)] for a in range(1, m - 1)]
+    return D, C, B, A
+
+
+def timeevompo_site(W: np.ndarray, delta: complex, alg: str = "WII") -> np.ndarray:
+    """W^I / W^II tensor of one Schur site tensor (m, d, n, d) -> (m-1, d, n-1, d).
+
+    Level 0 of the result carries D, levels 1.. the interior channels:
+    ``WI = [[1 + delta D, s C], [s B, A]]`` and for W^II, for every interior pair (a, b),
+    the first block column of ``exp(M)`` with M the 4 x 4 block operator on the
+    auxiliary states (0, c, b, bc): ``M[x, x] = delta D``, ``M[c, 0] = s C_b``,
+    ``M[b, 0] = s B_a``, ``M[bc, 0] = A_ab``, ``M[bc, c] = s B_a``, ``M[bc, b] = s C_b``,
+    ``s = sqrt(delta)``; ``W_D = E[0,0]``, ``W_C(b) = E[c,0]``, ``W_B(a) = E[b,0]``,
+    ``W_A(a,b) = E[bc,0]``."""
+    import scipy.linalg as sl
+    d = W.shape[1]
+    D, C, B, A = _schur_blocks(W)
+    kl, kr = len(B), len(C)
+    s = np.sqrt(complex(delta))
+    out = np.zeros((kl + 1, d, kr + 1, d), dtype=C128, order="F")
+    if alg == "WI":
+        out[0, :, 0, :] = np.eye(d) + delta * D
+        for b in range(kr):
+            out[0, :, b + 1, :] = s * C[b]
+        for a in range(kl):
+            out[a + 1, :, 0, :] = s * B[a]
+            for b in range(kr):
+                out[a + 1, :, b + 1, :] = A[a][b]
+        return out
+    Z = np.zeros((d, d), dtype=C128)
+
+    def block_exp(Cb, Ba, Aab):
+        M = np.zeros((4 * d, 4 * d), dtype=C128)
+        for x in range(4):
+            M[x * d:(x + 1) * d, x * d:(x + 1) * d] = delta * D
+        M[1 * d:2 * d, 0:d] = s * Cb
+        M[2 * d:3 * d, 0:d] = s * Ba
+        M[3 * d:4 * d, 0:d] = Aab
+        M[3 * d:4 * d, 1 * d:2 * d] = s * Ba
+        M[3 * d:4 * d, 2 * d:3 * d] = s * Cb
+        E = sl.expm(M)
+        return [E[x * d:(x + 1) * d, 0:d] for x in range(4)]
+    out[0, :, 0, :] = block_exp(Z, Z, Z)[0]
+    for b in range(kr):
+        out[0, :, b + 1, :] = block_exp(C[b], Z, Z)[1]
+    for a in range(kl):
+        out[a + 1, :, 0, :] = block_exp(Z, B[a], Z)[2]
+        for b in range(kr):
+            out[a + 1, :, b + 1, :] = block_exp(C[b], B[a], A[a][b])[3]
+    return out
+
+
+def timeevompo(H: SchurMPO, delta: complex, alg: str = "WII") -> List[np.ndarray]:
+    """``timeevompo(H::SparseIMPO, delta, WI()/WII())`` (``w1w2.jl:26-31``): the per-site
+    tensors of the dense time-evolution MPO approximating ``exp(delta H)``."""
+    return [timeevompo_site(W, delta, alg) for W in H.Ws]
+
+
+def mpo_ring(Ws: Sequence[np.ndarray], L: int) -> np.ndarray:
+    """Periodic-trace operator of an MPO on a ring of L sites (the MPO tensors repeated):
+    sum over the bond indices of W_1 W_2 ... W_L, a d^L x d^L matrix (site 1 slowest)."""
+    N = len(Ws)
+    W0 = Ws[0]
+    m, d = W0.shape[0], W0.shape[1]
+    # T[i, (out), (in), j]: running product with open first and last bonds
+    T = np.transpose(W0, (0, 1, 3, 2))  # (i, u, s, j)
+    for l in range(1, L):
+        Wl = Ws[l % N]
+        T = np.einsum("iabk,kuvj->iaubvj", T, np.transpose(Wl, (0, 1, 3, 2)))
+        i_, a, u, b, v, j = T.shape
+        T = T.reshape(i_, a * u, b * v, j)
+    return np.einsum("iabi->ab", T)
