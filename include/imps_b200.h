@@ -289,6 +289,13 @@ int imps_energy_dense(imps_envs* envs, const imps_mpo* mpo, imps_state* st, doub
  * complex; out receives nj interleaved complex values.  As in the reference, a later j
  * transfers through AR from the previous j + 1 on. */
 int imps_correlator(imps_state* st, const double* O1, const double* O2, int i, int nj, const int* js, double* out);
+/* Truncated thin SVD M = U diag(s) V^H of the host matrix M (m x n, column-major complex)
+ * by one-sided Jacobi on the device (the tsvd of the two-site splits; FiniteMPSAlgorithms
+ * `tsvd`, used at src/algorithms/groundstates/idmrg.jl:107-111): s descending, at most
+ * kmax (> 0, else min(m, n)) values kept and those above `cutoff` (at least one); U
+ * (m x k), s (k), V (n x k) caller-owned with room for min(m, n) columns; *k receives k. */
+int imps_svd(imps_ctx* ctx, int m, int n, const double* M, int kmax, double cutoff, double* U, double* s, double* V,
+             int* k);
 /* entanglement_spectrum(psi, loc) (src/observables/toolbox.jl:9-14) of bond `bond`
  * (0-based, bond l right of site l): the chi normalised squared singular values of C,
  * descending (one-sided Jacobi on the device); p holds chi doubles. */

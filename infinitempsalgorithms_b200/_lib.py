@@ -86,6 +86,7 @@ _SIGS = {
     "imps_energy_dense": (I32, [P, P, P, DP, DP]),
     "imps_correlator": (I32, [P, DP, DP, I32, I32, C.POINTER(I32), DP]),
     "imps_entanglement_spectrum": (I32, [P, I32, DP]),
+    "imps_svd": (I32, [P, I32, I32, DP, I32, D, DP, DP, DP, C.POINTER(I32)]),
     "imps_ctx_set_workspace_limit": (I32, [P, I64]),
     "imps_ctx_workspace_bytes": (I32, [P, C.POINTER(I64)]),
     "imps_ctx_counters_ext": (I32, [P, C.POINTER(I64), I32]),

@@ -27,7 +27,7 @@ __all__ = [
     "CanonicalIMPS", "randomimps", "random_site_tensors", "DMRGCache", "recalculate", "AC_hamiltonian",
     "C_hamiltonian", "fixedpoint", "integrate", "regauge", "calc_galerkin", "expectationvalue", "VUMPS",
     "IDMRG", "TDVP", "IterativeConvergenceInfo", "find_groundstate", "timestep", "time_evolve", "linsolve",
-    "qrpos", "lqpos", "push_env_left", "push_env_right", "push_mpo_left", "push_mpo_right",
+    "qrpos", "lqpos", "tsvd", "push_env_left", "push_env_right", "push_mpo_left", "push_mpo_right",
     "energy_gradient_mpo", "energy_gradient_AL", "coupling_gradient", "rrule_energy", "find_groundstate_batch",
     "DenseIMPO", "identityimpo", "timeevompo", "dominant_env", "correlator", "entanglement_spectrum", "renyi_entropy", "entropy",
 ]
@@ -681,6 +681,23 @@ def lqpos(M: np.ndarray, ctx: Optional[Context] = None):
     Q = np.zeros((k, n), complex, order="F")
     check(ctx.lib.imps_lqpos(ctx.h, m, n, dptr(M), dptr(Lf), dptr(Q)), ctx.h)
     return Lf, Q
+
+
+def tsvd(M: np.ndarray, kmax: int = 0, cutoff: float = 0.0, ctx: Optional[Context] = None):
+    """Truncated SVD ``M = U diag(s) V^H`` on the device (one-sided Jacobi): ``(U, s, V)``
+    with ``s`` descending, at most ``kmax`` values (all if 0) above ``cutoff``."""
+    ctx = ctx or default_context()
+    M = cbuf(M)
+    m, n = M.shape
+    r = min(m, n)
+    U = np.zeros((m, r), complex, order="F")
+    V = np.zeros((n, r), complex, order="F")
+    s = np.zeros(r)
+    k = C.c_int()
+    check(ctx.lib.imps_svd(ctx.h, m, n, dptr(M), int(kmax), float(cutoff), dptr(U), s.ctypes.data_as(L.DP),
+                           dptr(V), C.byref(k)), ctx.h)
+    kk = k.value
+    return np.asfortranarray(U[:, :kk]), s[:kk].copy(), np.asfortranarray(V[:, :kk])
 
 
 def regauge(AC: np.ndarray, Cm: np.ndarray, ctx: Optional[Context] = None) -> np.ndarray:

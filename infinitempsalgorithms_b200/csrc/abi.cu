@@ -947,6 +947,26 @@ int imps_correlator(imps_state* st, const double* O1, const double* O2, int i, i
   });
 }
 
+int imps_svd(imps_ctx* h, int m, int n, const double* A, int kmax, double cutoff, double* U, double* s, double* V,
+             int* k) {
+  if (!h || !A || !U || !s || !V || !k || m <= 0 || n <= 0) return IMPS_INVALID_ARG;
+  return guard(&h->c, [&] {
+    imps::Context* ctx = &h->c;
+    const int r = std::min(m, n);
+    imps::DevBuf& Ad = ctx->buf("abi_svd_a", (size_t)m * n * sizeof(imps::dcplx));
+    imps::DevBuf& Ud = ctx->buf("abi_svd_u", (size_t)m * r * sizeof(imps::dcplx));
+    imps::DevBuf& Vd = ctx->buf("abi_svd_v", (size_t)n * r * sizeof(imps::dcplx));
+    imps::upload(ctx, Ad.ptr, A, (size_t)m * n * sizeof(imps::dcplx));
+    std::vector<double> sv;
+    const int kk = imps::svd_thin(ctx, m, n, Ad.z(), m, kmax, cutoff, Ud.z(), sv, Vd.z());
+    imps::download(ctx, U, Ud.ptr, (size_t)m * kk * sizeof(imps::dcplx));
+    imps::download(ctx, V, Vd.ptr, (size_t)n * kk * sizeof(imps::dcplx));
+    std::copy(sv.begin(), sv.end(), s);
+    *k = kk;
+    return IMPS_OK;
+  });
+}
+
 int imps_entanglement_spectrum(imps_state* st, int bond, double* p) {
   if (!st || !p) return IMPS_INVALID_ARG;
   return guard(st->ctx, [&] {

@@ -44,7 +44,8 @@ __device__ __forceinline__ int rr_player(int pos, int r, int P) {
 // [[alpha, |gamma|], [|gamma|, beta]] applied to (u_a, e^{-i phi} u_b) makes them
 // orthogonal.  *rot counts the rotations performed (the convergence test of a sweep).
 __global__ void __launch_bounds__(kJacThreads) k_jacobi_round(int n, int ncol, int P, int r, dcplx* __restrict__ U,
-                                                          int64_t ldu, double tol, int* __restrict__ rot) {
+                                                          int64_t ldu, double tol, int* __restrict__ rot,
+                                                          dcplx* __restrict__ V, int nv, int64_t ldv) {
   __shared__ double sh[kJacThreads / 32];
   const int k = blockIdx.x;
   int a = rr_player(k, r, P), b = rr_player(P - 1 - k, r, P);
@@ -84,7 +85,32 @@ __global__ void __launch_bounds__(kJacThreads) k_jacobi_round(int n, int ncol, i
     // back to the original phase of column b: e^{i phi} y''
     ub[i] = make_double2(er * nyr - ei * nyi, er * nyi + ei * nyr);
   }
+  // the same rotation on the columns of V (right singular vectors), if requested
+  if (V) {
+    dcplx* va = V + ldv * (int64_t)a;
+    dcplx* vb = V + ldv * (int64_t)b;
+    for (int i = threadIdx.x; i < nv; i += kJacThreads) {
+      const dcplx x = va[i], y = vb[i];
+      const double ypr = er * y.x + ei * y.y, ypi = er * y.y - ei * y.x;
+      const double nxr = c * x.x - s * ypr, nxi = c * x.y - s * ypi;
+      const double nyr = s * x.x + c * ypr, nyi = s * x.y + c * ypi;
+      va[i] = make_double2(nxr, nxi);
+      vb[i] = make_double2(er * nyr - ei * nyi, er * nyi + ei * nyr);
+    }
+  }
   if (threadIdx.x == 0) atomicAdd(rot, 1);
+}
+
+// out[:, j] = scale_j * in[:, perm[j]] for j < k (column gather with optional scaling)
+__global__ void k_gather_cols(int rows, int k, const dcplx* __restrict__ in, int64_t ldi, const int* __restrict__ perm,
+                              const double* __restrict__ scale, dcplx* __restrict__ out, int64_t ldo) {
+  const int64_t tot = (int64_t)rows * k;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < tot; t += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(t % rows), j = (int)(t / rows);
+    const dcplx v = in[i + ldi * (int64_t)perm[j]];
+    const double f = scale ? scale[j] : 1.0;
+    out[i + ldo * (int64_t)j] = make_double2(v.x * f, v.y * f);
+  }
 }
 
 __global__ void k_col_norms2(int n, int ncol, const dcplx* __restrict__ U, int64_t ldu, double* __restrict__ out) {
@@ -120,7 +146,8 @@ std::vector<double> singular_values_sq(Context* ctx, int m, int n, const dcplx* 
   for (int sweep = 0; sweep < 60; ++sweep) {
     IMPS_CUDA(cudaMemsetAsync(flag.ptr, 0, sizeof(int), ctx->stream));
     for (int r = 0; r < P - 1; ++r) {
-      k_jacobi_round<<<P / 2, kJacThreads, 0, ctx->stream>>>(m, n, P, r, U.z(), m, tol, static_cast<int*>(flag.ptr));
+      k_jacobi_round<<<P / 2, kJacThreads, 0, ctx->stream>>>(m, n, P, r, U.z(), m, tol, static_cast<int*>(flag.ptr),
+                                                             nullptr, 0, 0);
       check(ctx);
     }
     int rot = 0;
@@ -133,6 +160,68 @@ std::vector<double> singular_values_sq(Context* ctx, int m, int n, const dcplx* 
   download(ctx, s2.data(), nr.ptr, n * sizeof(double));
   std::sort(s2.begin(), s2.end(), [](double x, double y) { return x > y; });
   return s2;
+}
+
+int svd_thin(Context* ctx, int m, int n, const dcplx* A, int64_t lda, int kmax, double cutoff, dcplx* U,
+             std::vector<double>& s, dcplx* V) {
+  IMPS_REQUIRE(m > 0 && n > 0, IMPS_INVALID_ARG, "svd: empty matrix");
+  if (m < n) {
+    // A = (A^H)^H: the SVD of A^H with the roles of U and V exchanged
+    DevBuf& AH = ctx->buf("svd_ah", (size_t)m * n * sizeof(dcplx));
+    zconj_transpose(ctx, m, n, A, lda, AH.z(), n);
+    DevBuf& Ut = ctx->buf("svd_ut", (size_t)n * std::min(m, kmax > 0 ? kmax : m) * sizeof(dcplx));
+    const int k = svd_thin(ctx, n, m, AH.z(), n, kmax, cutoff, Ut.z(), s, U);
+    // V = U' (n x k) of the transposed problem
+    zcopy2d(ctx, n, k, Ut.z(), n, V, n);
+    return k;
+  }
+  const int P = n + (n & 1);
+  DevBuf& W = ctx->buf("svd_w", (size_t)m * P * sizeof(dcplx));
+  DevBuf& Vw = ctx->buf("svd_v", (size_t)n * P * sizeof(dcplx));
+  DevBuf& flag = ctx->buf("jac_flag", 64);
+  DevBuf& nr = ctx->buf("jac_norms", (size_t)P * sizeof(double));
+  zcopy2d(ctx, m, n, A, lda, W.z(), m);
+  zset_identity(ctx, n, Vw.z(), n, 1.0);
+  ScopedTimer tm(ctx, "jacobi_svd", 0.0);
+  const double tol = 1e-15 * std::sqrt((double)m);
+  for (int sweep = 0; sweep < 60; ++sweep) {
+    IMPS_CUDA(cudaMemsetAsync(flag.ptr, 0, sizeof(int), ctx->stream));
+    for (int r = 0; r < P - 1; ++r) {
+      k_jacobi_round<<<P / 2, kJacThreads, 0, ctx->stream>>>(m, n, P, r, W.z(), m, tol, static_cast<int*>(flag.ptr),
+                                                             Vw.z(), n, n);
+      check(ctx);
+    }
+    int rot = 0;
+    download(ctx, &rot, flag.ptr, sizeof(int));
+    if (rot == 0) break;
+  }
+  k_col_norms2<<<n, kJacThreads, 0, ctx->stream>>>(m, n, W.z(), m, nr.d());
+  check(ctx);
+  std::vector<double> n2(n);
+  download(ctx, n2.data(), nr.ptr, n * sizeof(double));
+  std::vector<int> perm(n);
+  for (int j = 0; j < n; ++j) perm[j] = j;
+  std::stable_sort(perm.begin(), perm.end(), [&](int x, int y) { return n2[x] > n2[y]; });
+  int k = kmax > 0 ? std::min(kmax, n) : n;
+  while (k > 1 && std::sqrt(std::max(n2[perm[k - 1]], 0.0)) <= cutoff) --k;
+  s.resize(k);
+  std::vector<double> inv(k);
+  for (int j = 0; j < k; ++j) {
+    s[j] = std::sqrt(std::max(n2[perm[j]], 0.0));
+    inv[j] = s[j] > 0.0 ? 1.0 / s[j] : 0.0;
+  }
+  DevBuf& pb = ctx->buf("svd_perm", (size_t)k * (sizeof(int) + sizeof(double)));
+  int* pd = static_cast<int*>(pb.ptr);
+  double* sd = reinterpret_cast<double*>(static_cast<char*>(pb.ptr) + (size_t)k * sizeof(int));
+  upload(ctx, pd, perm.data(), (size_t)k * sizeof(int));
+  upload(ctx, sd, inv.data(), (size_t)k * sizeof(double));
+  auto grid = [](int64_t t) { return (int)std::max<int64_t>(1, std::min<int64_t>((t + 255) / 256, 148 * 8)); };
+  // U = W[:, perm] / s (columns of exactly zero singular value stay zero), V = Vw[:, perm]
+  k_gather_cols<<<grid((int64_t)m * k), 256, 0, ctx->stream>>>(m, k, W.z(), m, pd, sd, U, m);
+  check(ctx);
+  k_gather_cols<<<grid((int64_t)n * k), 256, 0, ctx->stream>>>(n, k, Vw.z(), n, pd, nullptr, V, n);
+  check(ctx);
+  return k;
 }
 
 std::vector<double> entanglement_spectrum(Context* ctx, imps_state* st, int bond) {

@@ -9,6 +9,11 @@ namespace imps {
 
 // Squared singular values (descending) of the m x n matrix A, by one-sided Jacobi.
 std::vector<double> singular_values_sq(Context* ctx, int m, int n, const dcplx* A, int64_t lda);
+// Thin SVD A = U diag(s) V^H by one-sided Jacobi (descending s), truncated to at most
+// kmax (> 0) values and to those above `cutoff` (at least one kept); U (m x k), V (n x k)
+// column-major with leading dimensions m and n.  Returns k.
+int svd_thin(Context* ctx, int m, int n, const dcplx* A, int64_t lda, int kmax, double cutoff, dcplx* U,
+             std::vector<double>& s, dcplx* V);
 // entanglement_spectrum(psi, loc): normalised squared Schmidt values of bond `bond` (0-based).
 std::vector<double> entanglement_spectrum(Context* ctx, imps_state* st, int bond);
 // dominant_env([W,] psi; side) into out (D x w x D, unit norm); mpo == nullptr: identity channel.

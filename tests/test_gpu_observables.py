@@ -99,3 +99,22 @@ def test_entanglement_spectrum_against_lapack(ctx, D, seed):
         assert np.max(np.abs(p - po)) < 1e-13
         assert abs(imps.entropy(psi, loc) - O.entropy(opsi, loc)) < 1e-11
         assert abs(imps.entropy(psi, loc, alpha=2.0) - O.entropy(opsi, loc, alpha=2.0)) < 1e-11
+
+
+@pytest.mark.parametrize("m,n,kmax", [(20, 7, 0), (7, 20, 0), (64, 64, 10), (300, 120, 0), (33, 1, 0)])
+def test_tsvd_against_lapack(ctx, m, n, kmax):
+    rng = np.random.default_rng(m + n)
+    M = rng.standard_normal((m, n)) + 1j * rng.standard_normal((m, n))
+    U, s, V = imps.tsvd(M, kmax, ctx=ctx)
+    so = np.linalg.svd(M, compute_uv=False)
+    k = len(s)
+    assert k == (kmax if kmax else min(m, n))
+    assert np.allclose(s, so[:k], rtol=1e-12, atol=1e-12 * so[0])
+    assert np.linalg.norm(U.conj().T @ U - np.eye(k)) < 1e-12 * k
+    assert np.linalg.norm(V.conj().T @ V - np.eye(k)) < 1e-12 * k
+    if kmax == 0:
+        assert np.linalg.norm((U * s) @ V.conj().T - M) < 1e-12 * np.linalg.norm(M)
+    else:
+        # best rank-k approximation error = the discarded singular values
+        err = np.linalg.norm((U * s) @ V.conj().T - M)
+        assert abs(err - np.linalg.norm(so[k:])) < 1e-10 * np.linalg.norm(M)
