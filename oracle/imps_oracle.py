@@ -58,6 +58,7 @@ __all__ = [
     "dominant_env", "normalize_envs", "build_envs_dense", "expectationvalue_dense", "apply_local", "correlator",
     "entanglement_spectrum", "renyi_entropy", "entropy",
     "timeevompo", "timeevompo_site", "mpo_ring",
+    "IDMRG2", "ac2_apply", "ac2", "idmrg2_split", "idmrg2_sweep", "idmrg2_groundstate",
 ]
 
 C128 = np.complex128
@@ -1711,3 +1712,154 @@ def mpo_ring(Ws: Sequence[np.ndarray], L: int) -> np.ndarray:
         i_, a, u, b, v, j = T.shape
         T = T.reshape(i_, a * u, b * v, j)
     return np.einsum("iabi->ab", T)
+
+
+# --------------------------------------------------------------------------
+# Two-site IDMRG (IDMRG2): src/algorithms/groundstates/idmrg.jl:90-235 and the two-site
+# effective Hamiltonian src/algorithms/groundstates/effective.jl:113-197.  Sites 0-based
+# (reference site pos = p + 1); the truncation is ``truncdim(D)`` (keep at most D
+# singular values), the reference's ``tsvd`` + ``normalize!(s)`` split.
+# --------------------------------------------------------------------------
+@dataclass
+class IDMRG2:
+    """``IDMRG2`` (``src/algorithms/algdefs.jl:106-116``) with ``trunc = truncdim(D)``."""
+    D: int = Defaults.D
+    tol: float = Defaults.tol
+    maxiter: int = Defaults.maxiter
+    alg_gauge: object = field(default_factory=alg_gauge)
+    alg_eigsolve: object = field(default_factory=alg_eigsolve)
+
+
+def ac2_apply(GL, W1, W2, GR, x):
+    """``MPO_AC2_Hamiltonian`` action (``effective.jl:160-197``):
+    ``y[b,u1,u2,c] = sum GL[b,w1,a] x[a,s1,s2,bb] W1[w1,u1,w2,s1] W2[w2,u2,wr,s2] GR[bb,wr,c]``."""
+    Dl, d1, d2, Dr = x.shape
+    m = W1.shape[0]
+    T1 = freshape(freshape(GL, (Dl * m, Dl)) @ freshape(x, (Dl, d1 * d2 * Dr)), (Dl, m, d1, d2, Dr))
+    T2 = np.tensordot(T1, W1, axes=([1, 2], [0, 3]))        # [b, s2, bb, u1, w2]
+    T3 = np.tensordot(T2, W2, axes=([4, 1], [0, 3]))        # [b, bb, u1, u2, wr]
+    return np.asfortranarray(np.tensordot(T3, GR, axes=([1, 4], [0, 1])))
+
+
+def ac2(psi: CanonicalIMPS, p: int, kind: str = "ACAR") -> np.ndarray:
+    """``AC2(psi, pos; kind)`` (``effective.jl:138-152``), 0-based ``p`` (periodic)."""
+    N = len(psi)
+    p %= N
+    q = (p + 1) % N
+    A1, A2 = (psi.AC[p], psi.AR[q]) if kind == "ACAR" else (psi.AL[p], psi.AC[q])
+    return np.asfortranarray(np.einsum("asm,mtb->astb", A1, A2))
+
+
+def idmrg2_split(x2: np.ndarray, D: int):
+    """``_idmrg2_split`` (``idmrg.jl:107-111``): SVD of the (Dl d1) x (d2 Dr) matrix, the
+    ``D`` largest values kept and normalised; returns ``(al, c, ar)``."""
+    Dl, d1, d2, Dr = x2.shape
+    U, S, Vh = np.linalg.svd(freshape(x2, (Dl * d1, d2 * Dr)), full_matrices=False)
+    k = min(D, len(S))
+    s = S[:k] / np.linalg.norm(S[:k])
+    al = np.asfortranarray(freshape(U[:, :k], (Dl, d1, k)))
+    ar = np.asfortranarray(freshape(Vh[:k, :], (k, d2, Dr)))
+    return al, np.diag(s).astype(C128), ar
+
+
+def _div_tail(A, C):
+    """``A / C`` on the last bond (``X C = A``)."""
+    Dl, d, Dr = A.shape
+    Xm = np.linalg.solve(C.T, freshape(A, (Dl * d, Dr)).T).T
+    return np.asfortranarray(freshape(Xm, (Dl, d, C.shape[1])))
+
+
+def _frontdiv(C, A):
+    """``C \\ A`` on the first bond."""
+    Dl, d, Dr = A.shape
+    Xm = np.linalg.solve(C, freshape(A, (Dl, d * Dr)))
+    return np.asfortranarray(freshape(Xm, (C.shape[1], d, Dr)))
+
+
+def idmrg2_sweep(psi: CanonicalIMPS, H: SchurMPO, envs: DMRGCache, ea: dict, D: int):
+    """``_localupdate_sweep_idmrg2!`` (``idmrg.jl:113-185``); returns ``(C_old, E)``."""
+    N = len(psi)
+    AL, AR, Cs, AC = psi.AL, psi.AR, psi.C, psi.AC
+
+    def tl(s):
+        s %= N
+        envs.lefts[s] = push_mpo_left(envs.lefts[s - 1], H[s - 1], AL[s - 1])
+
+    def tr(s):
+        s %= N
+        q = (s + 1) % N
+        envs.rights[s] = push_mpo_right(envs.rights[q], H[q], AR[q])
+
+    def solve(p, kind):
+        q = (p + 1) % N
+        GL, W1, W2, GR = envs.lefts[p % N], H[p % N], H[q], envs.rights[q]
+        E, x, _ = lanczos_eigsolve(lambda v: ac2_apply(GL, W1, W2, GR, v), ac2(psi, p, kind), ea["tol"],
+                                   ea["krylovdim"], ea["maxiter"], ea["eager"])
+        return E, x
+
+    for p in range(N - 1):
+        _, x = solve(p, "ACAR")
+        al, c, ar = idmrg2_split(x, D)
+        AL[p], Cs[p], AR[p + 1] = al, c, ar
+        AC[p + 1] = _mulCA(c, ar)
+        tl(p + 1)
+        tr(p)
+    AL[N - 1] = _div_tail(AC[N - 1], Cs[N - 1])
+    AC[0] = _mulAL(AL[0], Cs[0])
+    _, x = solve(N - 1, "ALAC")
+    al, c, ar = idmrg2_split(x, D)
+    AL[N - 1], Cs[N - 1], AR[0] = al, c, ar
+    AC[N - 1] = _mulAL(al, c)
+    AC[0] = _mulCA(c, ar)
+    AL[0] = _div_tail(AC[0], Cs[0])
+    C_old = c.copy()
+    tl(0)
+    tr(N - 1)
+    for p in range(N - 2, -1, -1):
+        _, x = solve(p, "ALAC")
+        al, c, ar = idmrg2_split(x, D)
+        AL[p] = al
+        AC[p] = _mulAL(al, c)
+        Cs[p] = c
+        AR[p + 1] = ar
+        AC[p + 1] = _mulCA(c, ar)
+        tl(p + 1)
+        tr(p)
+    AC[N - 1] = _mulCA(Cs[N - 2], AR[N - 1])
+    AR[0] = _frontdiv(Cs[N - 1], AC[0])
+    E, x = solve(N - 1, "ACAR")
+    al, c, ar = idmrg2_split(x, D)
+    AL[N - 1], Cs[N - 1], AR[0] = al, c, ar
+    AR[N - 1] = _frontdiv(Cs[N - 2], _mulAL(al, c))
+    AC[0] = _mulCA(c, ar)
+    tl(0)
+    tr(N - 1)
+    return C_old, E
+
+
+def idmrg2_groundstate(psi0: CanonicalIMPS, H: SchurMPO, alg: IDMRG2, envs: Optional[DMRGCache] = None):
+    """``find_groundstate(psi0, H, ::IDMRG2)`` (``idmrg.jl:203-235``)."""
+    psi = psi0.copy()
+    N = len(psi)
+    if N < 2:
+        raise ValueError("IDMRG2 requires unit cell length >= 2")
+    if envs is None:
+        envs = build_envs(psi, H)
+    envs = DMRGCache([x.copy(order="F") for x in envs.lefts], [x.copy(order="F") for x in envs.rights])
+    eps = calc_galerkin(psi, H, envs)
+    losses = [eps]
+    converged = False
+    it = 0
+    E = None
+    for it in range(1, alg.maxiter + 1):
+        ea = updatetol(alg.alg_eigsolve, it - 1, eps)
+        C_old, E = idmrg2_sweep(psi, H, envs, ea, alg.D)
+        eps = _fnorm(psi.C[N - 1] - C_old)
+        losses.append(eps)
+        if eps <= alg.tol:
+            converged = True
+            break
+    ag = updatetol(alg.alg_gauge, it, eps)
+    psi2 = canonical_from_sites([psi.AR[l] for l in range(N)], tol=ag["tol"], maxiter=ag["maxiter"])
+    envs2 = build_envs(psi2, H)
+    return psi2, envs2, dict(niter=it, converged=converged, losses=losses, itererr=losses[-1], E=E)
