@@ -354,6 +354,20 @@ int imps_tdvp_step(imps_envs* envs, const imps_mpo* mpo, imps_state* st, double 
  * last eigenvalue in *E and ||C[0] - C_old|| in *eps. */
 int imps_idmrg_sweep(imps_envs* envs, const imps_mpo* mpo, imps_state* st, double tol, int krylovdim,
                      int maxiter, int eager, double* E, double* eps);
+/* _localupdate_sweep_idmrg2! (src/algorithms/groundstates/idmrg.jl:113-185) with
+ * trunc = truncdim(D) (_idmrg2_split, idmrg.jl:107-111): two-site windows L->R as :ACAR,
+ * the wrap window as :ALAC, R->L as :ALAC, the closing window as :ACAR.  Bond dimensions
+ * change in place (k = min(D, Dl d1, d2 Dr) at every split; read them back with
+ * imps_state_bonds).  Requires N >= 2 (ArgumentError otherwise).  *E = eigenvalue of the
+ * closing window, *eps = ||C[0] - C_old|| (diagonals zero-padded when their sizes differ;
+ * the reference's norm of a difference assumes equal sizes).  FP64 throughout. */
+int imps_idmrg2_sweep(imps_envs* envs, const imps_mpo* mpo, imps_state* st, int D, double tol, int krylovdim,
+                      int maxiter, int eager, double* E, double* eps);
+/* y = AC2_hamiltonian(p) * x for the window (p, p+1), 0-based p, x and y (Dl, d1, d2, Dr)
+ * column-major on the host (MPO_AC2_Hamiltonian action, effective.jl:160-197). */
+int imps_ac2_apply(imps_envs* envs, const imps_mpo* mpo, int p, const double* x, double* y);
+/* chi[l] = bond dimension right of site l, l = 0..N-1 (bonddim(psi, l+1)). */
+int imps_state_bonds(const imps_state* st, int* chi);
 
 #ifdef __cplusplus
 }

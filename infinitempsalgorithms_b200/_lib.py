@@ -143,6 +143,9 @@ _SIGS = {
                                     C.POINTER(VumpsInfo), C.POINTER(I32), I32]),
     "imps_tdvp_step": (I32, [P, P, P, D, D, D, I32, I32, D, I32, C.POINTER(KrylovInfo)]),
     "imps_idmrg_sweep": (I32, [P, P, P, D, I32, I32, I32, DP, DP]),
+    "imps_idmrg2_sweep": (I32, [P, P, P, I32, D, I32, I32, I32, DP, DP]),
+    "imps_ac2_apply": (I32, [P, P, I32, DP, DP]),
+    "imps_state_bonds": (I32, [P, C.POINTER(I32)]),
 }
 
 _lib = None

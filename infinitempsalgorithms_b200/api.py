@@ -26,7 +26,7 @@ __all__ = [
     "SparseIMPO", "tfim_hamiltonian", "heisenberg_hamiltonian", "hubbard_hamiltonian", "PeriodicVector",
     "CanonicalIMPS", "randomimps", "random_site_tensors", "DMRGCache", "recalculate", "AC_hamiltonian",
     "C_hamiltonian", "fixedpoint", "integrate", "regauge", "calc_galerkin", "expectationvalue", "VUMPS",
-    "IDMRG", "TDVP", "IterativeConvergenceInfo", "find_groundstate", "timestep", "time_evolve", "linsolve",
+    "IDMRG", "IDMRG2", "ac2_apply", "TDVP", "IterativeConvergenceInfo", "find_groundstate", "timestep", "time_evolve", "linsolve",
     "qrpos", "lqpos", "tsvd", "push_env_left", "push_env_right", "push_mpo_left", "push_mpo_right",
     "energy_gradient_mpo", "energy_gradient_AL", "coupling_gradient", "rrule_energy", "find_groundstate_batch",
     "DenseIMPO", "identityimpo", "timeevompo", "dominant_env", "correlator", "entanglement_spectrum", "renyi_entropy", "entropy",
@@ -947,6 +947,19 @@ class IDMRG:
 
 
 @dataclass
+class IDMRG2:
+    """``IDMRG2(; trunc, tol, maxiter, verbosity, alg_gauge, alg_eigsolve, finalize)``
+    (``src/algorithms/algdefs.jl:85-116``) with ``trunc = truncdim(D)``."""
+    D: int = Defaults.D
+    tol: float = Defaults.tol
+    maxiter: int = Defaults.maxiter
+    verbosity: int = Defaults.verbosity
+    alg_gauge: object = field(default_factory=Defaults.alg_gauge)
+    alg_eigsolve: object = field(default_factory=Defaults.alg_eigsolve)
+    finalize: Optional[Callable] = None
+
+
+@dataclass
 class TDVP:
     """``TDVP(; integrator, alg_gauge, verbosity, finalize)``."""
     integrator: dict = field(default_factory=Defaults.alg_expsolve)
@@ -981,6 +994,8 @@ def find_groundstate(psi0, H: SparseIMPO, alg=None, envs: Optional[DMRGCache] = 
         raise ValueError("only :SR is supported")
     if isinstance(alg, IDMRG):
         return _find_groundstate_idmrg(psi0, H, alg, envs)
+    if isinstance(alg, IDMRG2):
+        return _find_groundstate_idmrg2(psi0, H, alg, envs)
     alg = alg or VUMPS()
     psi = psi0.copy()
     ctx = psi.ctx
@@ -1073,6 +1088,62 @@ def find_groundstate_batch(psi0s: Sequence[CanonicalIMPS], Hs: Sequence[SparseIM
         active = [i for i in active if not converged[i] and iters[i] < alg.maxiter]
     return [(psis[i], envss[i], IterativeConvergenceInfo(iters[i], converged[i], losses[i], losses[i][-1]))
             for i in range(n)]
+
+
+def _refresh_bonds(psi):
+    chi = (C.c_int * psi.N)()
+    check(psi.ctx.lib.imps_state_bonds(psi.h, chi), psi.ctx.h)
+    psi.chi = list(chi)
+
+
+def ac2_apply(envs: "DMRGCache", H: SparseIMPO, pos: int, x: np.ndarray) -> np.ndarray:
+    """``AC2_hamiltonian(pos, psi, H, psi, envs) * x`` for the window ``(pos, pos+1)``
+    (1-based ``pos``, periodic; ``effective.jl:160-197``); ``x`` is ``(Dl, d1, d2, Dr)``."""
+    ctx = envs.ctx
+    xb = cbuf(x)
+    y = np.zeros(xb.shape, complex, order="F")
+    check(ctx.lib.imps_ac2_apply(envs.h, H.handle(ctx), (pos - 1) % envs.N, dptr(xb), dptr(y)), ctx.h)
+    return y
+
+
+def _find_groundstate_idmrg2(psi0, H, alg: IDMRG2, envs=None):
+    """``find_groundstate(psi0, H, ::IDMRG2)`` (``idmrg.jl:203-235``): two-site sweeps with
+    ``truncdim(alg.D)``; the bond dimensions follow the truncation.  Requires N >= 2."""
+    if len(psi0) < 2:
+        raise L.ArgumentError(L.IMPS_INVALID_ARG, "IDMRG2 requires unit cell length >= 2")
+    if isinstance(H, DenseIMPO):
+        raise NotImplementedError("IDMRG2 runs on the Schur (SparseIMPO) channel")
+    psi = psi0.copy()
+    ctx = psi.ctx
+    Hh = H.handle(ctx)
+    if envs is None:
+        envs = DMRGCache(psi0, H)
+    eps = calc_galerkin(psi, H, envs)
+    losses = [eps]
+    converged = False
+    it = 0
+    for it in range(1, alg.maxiter + 1):
+        ea = updatetol(alg.alg_eigsolve, it - 1, eps)
+        E, err = C.c_double(), C.c_double()
+        check(ctx.lib.imps_idmrg2_sweep(envs.h, Hh, psi.h, int(alg.D), ea["tol"], ea["krylovdim"], ea["maxiter"],
+                                        int(ea["eager"]), C.byref(E), C.byref(err)), ctx.h)
+        _refresh_bonds(psi)
+        envs.chi = list(psi.chi)
+        if alg.finalize is not None:
+            psi, envs = alg.finalize(it, psi, H, envs)
+        eps = err.value
+        losses.append(eps)
+        if alg.verbosity > 0:
+            _logiter("IDMRG2", it, eps, f=E.value)
+        if eps <= alg.tol:
+            converged = True
+            break
+    ag = updatetol(alg.alg_gauge, it, eps)
+    ARs = [psi.get(L.IMPS_AR, l) for l in range(psi.N)]
+    psi2 = CanonicalIMPS.from_sites(ARs, tol=ag["tol"], maxiter=ag["maxiter"], ctx=ctx)
+    envs2 = DMRGCache(psi2, H, build=False)
+    envs2.build(psi2, H, warm=False)
+    return psi2, envs2, IterativeConvergenceInfo(it, converged, losses, losses[-1])
 
 
 def _find_groundstate_idmrg(psi0, H, alg: IDMRG, envs=None):

@@ -1086,4 +1086,38 @@ int imps_idmrg_sweep(imps_envs* E, const imps_mpo* mpo, imps_state* st, double t
   });
 }
 
+int imps_idmrg2_sweep(imps_envs* E, const imps_mpo* mpo, imps_state* st, int D, double tol, int krylovdim,
+                      int maxiter, int eager, double* Eout, double* eps) {
+  if (!E || !mpo || !st || D <= 0 || tol < 0 || krylovdim <= 0 || maxiter <= 0) return IMPS_INVALID_ARG;
+  return guard(E->ctx, [&] {
+    imps::idmrg2_sweep(E->ctx, E, mpo, st, D, tol, krylovdim, maxiter, eager != 0, Eout, eps);
+    return IMPS_OK;
+  });
+}
+
+int imps_ac2_apply(imps_envs* E, const imps_mpo* mpo, int p, const double* x, double* y) {
+  if (!E || !mpo || !x || !y || p < 0 || p >= E->N) return IMPS_INVALID_ARG;
+  return guard(E->ctx, [&] {
+    imps::Context* ctx = E->ctx;
+    IMPS_REQUIRE(E->N >= 2, IMPS_INVALID_ARG, "two-site window needs unit cell length >= 2");
+    const int q = (p + 1) % E->N;
+    const size_t n = (size_t)E->Dl[p] * mpo->sites[p % mpo->N].d * mpo->sites[q % mpo->N].d * E->Dr[q];
+    imps::DevBuf& xd = ctx->buf("abi_ac2_x", n * sizeof(imps::dcplx));
+    imps::DevBuf& yd = ctx->buf("abi_ac2_y", n * sizeof(imps::dcplx));
+    imps::upload(ctx, xd.ptr, x, n * sizeof(imps::dcplx));
+    {
+      imps::Fp64Scope fp64(ctx);
+      imps::ac2_apply(ctx, E, mpo, p, xd.z(), yd.z());
+    }
+    imps::download(ctx, y, yd.ptr, n * sizeof(imps::dcplx));
+    return IMPS_OK;
+  });
+}
+
+int imps_state_bonds(const imps_state* st, int* chi) {
+  if (!st || !chi) return IMPS_INVALID_ARG;
+  for (int l = 0; l < st->N; ++l) chi[l] = st->chi[l];
+  return IMPS_OK;
+}
+
 }  // extern "C"

@@ -26,4 +26,9 @@ KrylovResult tdvp_step(Context* ctx, imps_envs* E, const imps_mpo* H, imps_state
                        int maxiter, double gauge_tol, int gauge_maxiter);
 void idmrg_sweep(Context* ctx, imps_envs* E, const imps_mpo* H, imps_state* st, double tol, int kdim, int maxiter,
                  bool eager, double* Eout, double* epsout);
+// two-site IDMRG (idmrg2.cu): y = AC2 Hamiltonian of window (p, p+1) applied to x (Dl, d1, d2, Dr)
+void ac2_apply(Context* ctx, const imps_envs* E, const imps_mpo* H, int p, const dcplx* x, dcplx* y);
+// one _localupdate_sweep_idmrg2! with truncdim(D); bond dimensions of st and E change in place
+void idmrg2_sweep(Context* ctx, imps_envs* E, const imps_mpo* H, imps_state* st, int D, double tol, int kdim,
+                  int maxiter, bool eager, double* Eout, double* epsout);
 }  // namespace imps
