@@ -8,19 +8,21 @@
 // the trailing columns updated with H^H), so R and Q agree with a LAPACK QR up to
 // the final phase fix Q[:, i] *= ph_i, R[i, :] *= conj(ph_i), ph_i = R_ii / |R_ii|.
 //
-// Blocked right-looking algorithm over panels of NB columns:
+// Two-level blocked right-looking algorithm:
 //  * k_qr_panel: one thread-block cluster of QR_CL CTAs factors the panel
-//    A[p:m, p:p+b].  Each thread keeps RPT rows of the panel in registers for the
-//    whole panel; per column the cluster reduces ||x||^2 (one value) and then the
-//    NB-1 inner products needed both for the trailing columns of the panel and for
-//    the compact-WY factor T (LAPACK zlarft, T[0:c, c] = -tau_c T[0:c, 0:c] V^H v_c),
-//    each through distributed shared memory after one cluster barrier.  The kernel
-//    writes R (upper part of A), V (explicit, unit diagonal, zeros above), tau and T.
-//  * the trailing matrix A2 = A[p:m, p+b:n] <- (I - V T V^H)^H A2 = A2 - V T^H (V^H A2),
-//    FP64 GEMMs on the DMMA engine; the long-K product V^H A2 is split into row
-//    chunks (one batched GEMM) and summed in a fixed order.
-//  * Q = H_1 ... H_k [I; 0] by the same block reflectors applied backwards:
-//    Q[p:m, p:k] <- (I - V T V^H) Q[p:m, p:k].
+//    A[p:m, p:p+b] (b <= 16), the panel rows staged in shared memory.  Per column a
+//    single cluster reduction (distributed shared memory after one cluster barrier)
+//    gives ||x||^2, the inner products with the trailing panel columns and those with
+//    the earlier reflectors needed for the compact-WY factor T (LAPACK zlarft,
+//    T[0:c, c] = -tau_c T[0:c, 0:c] V^H v_c).  The kernel writes R (upper part of A),
+//    V (explicit, unit diagonal, zeros above), tau and T.
+//  * inner panels update only the rest of their outer block of QR_NBO columns; the
+//    outer block's T is merged from the panels' factors (k_merge_t, with G = V^H V),
+//    and the trailing matrix A2 <- (I - V T V^H)^H A2 = A2 - (V T^H) (A2^H V)^H is updated
+//    once per outer block by FP64 GEMMs on the DMMA engine (the long-K product A2^H V
+//    split into row chunks, one batched GEMM, summed in a fixed order).
+//  * Q = H_1 ... H_k [I; 0] by the outer block reflectors applied backwards:
+//    Q[P:m, P:k] <- (I - V T V^H) Q[P:m, P:k].
 // LQpos is QRpos of the conjugate transpose.
 #include <algorithm>
 
@@ -36,7 +38,9 @@ constexpr int QR_CL = 8;     // CTAs per cluster (portable cluster size)
 constexpr int QR_NT = 512;   // threads per CTA
 constexpr int QR_G = QR_CL * QR_NT;
 constexpr int QR_NBMAX = 16;
-constexpr int QR_KC = 256;   // rows per split-K chunk of the V^H X products
+constexpr int QR_NBO = 64;   // outer block: columns per compact-WY trailing update
+constexpr size_t QR_PANEL_SMEM = (size_t)QR_NBMAX * QR_NT * sizeof(dcplx);  // NB RPT = 16 for every panel kind
+constexpr int QR_MAXCHUNK = 32;  // most row chunks of a split-K X^H V product
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -51,12 +55,12 @@ __device__ __forceinline__ uint32_t cluster_rank() {
 __device__ __forceinline__ void cluster_sync() {
   asm volatile("barrier.cluster.arrive.release.aligned;\n barrier.cluster.wait.acquire.aligned;" ::: "memory");
 }
-__device__ __forceinline__ double ld_peer(const double* local, uint32_t rank) {
+// store v into the same shared variable of CTA `rank` of the cluster (made visible to
+// that CTA by the next cluster barrier's release / acquire)
+__device__ __forceinline__ void st_peer(double* local, uint32_t rank, double v) {
   uint32_t a;
   asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(a) : "r"(smem_addr(local)), "r"(rank));
-  double v;
-  asm volatile("ld.shared::cluster.f64 %0, [%1];" : "=d"(v) : "r"(a) : "memory");
-  return v;
+  asm volatile("st.shared::cluster.f64 [%0], %1;" ::"r"(a), "d"(v) : "memory");
 }
 
 __device__ __forceinline__ dcplx cmul(dcplx a, dcplx b) {
@@ -66,164 +70,170 @@ __device__ __forceinline__ dcplx cmulc(dcplx a, dcplx b) {  // conj(a) * b
   return make_double2(fma(a.x, b.x, a.y * b.y), fma(a.x, b.y, -a.y * b.x));
 }
 
+// Sum of val[s] over the 32 lanes of a warp for NV slots by a reduce-scatter: log2(NV)
+// exchange rounds of halving width (NV - 1 shuffles in all), then plain rounds over the
+// lanes that share a slot.  Returns the warp total of slot lane / (32 / NV).
+template <int NV>
+__device__ __forceinline__ double warp_reduce_scatter(double (&val)[NV], int lane) {
+  int half = NV;
+#pragma unroll
+  for (int o = 16; o >= 32 / NV; o >>= 1) {
+    half >>= 1;
+    const bool up = (lane & o) != 0;
+#pragma unroll
+    for (int v = 0; v < NV / 2; ++v) {
+      if (v < half) {
+        const double send = up ? val[v] : val[v + half];
+        const double keep = up ? val[v + half] : val[v];
+        val[v] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+      }
+    }
+  }
+  double r = val[0];
+#pragma unroll
+  for (int o = 32 / NV / 2; o >= 1; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+  return r;
+}
+
 // Householder factorization of the panel A[0:R, 0:b] (lda), b <= NB.  Row il of the
-// panel is held by cluster thread g = rank * QR_NT + tid with il = g + k QR_G, k < RPT.
-// Outputs: A (R above/on the diagonal, v below), V (R x b, ldv: v with unit diagonal
-// and zeros above), tau[0:b], T (b x b, ldt, upper triangular).
+// panel belongs to cluster thread g = rank * QR_NT + tid with il = g + k QR_G, k < RPT,
+// and lives in shared memory (NB RPT QR_NT complex = 128 KiB per CTA).
+// One cluster reduction per column: ||x_c below||^2, d_j = x_c^H x_j (j > c, trailing
+// panel columns) and e_l = V_l^H x_c (l < c, for T), all over the rows below c, together
+// with row c of the panel (held by thread c of CTA 0).  With v = [1; scale x_c below]:
+//   v^H x_j = x_j[c] + conj(scale) d_j,   V_l^H v = conj(V_l[c]) + scale e_l.
+// Outputs: A (R above/on the diagonal, v below), V (R x b, ldv: v with unit diagonal and
+// zeros above; the zabove rows before row 0 are zeroed too), tau[0:b], T (b x b, ldt).
 template <int NB, int RPT>
 __global__ void __cluster_dims__(QR_CL, 1, 1) __launch_bounds__(QR_NT, 1)
-    k_qr_panel(int R, int b, dcplx* __restrict__ A, int64_t lda, dcplx* __restrict__ V, int64_t ldv,
+    k_qr_panel(int R, int b, int zabove, dcplx* __restrict__ A, int64_t lda, dcplx* __restrict__ V, int64_t ldv,
                dcplx* __restrict__ tau, dcplx* __restrict__ T, int ldt) {
-  __shared__ double red_ssq[2];              // CTA partial of ||x||^2, by column parity
-  __shared__ double alpha_sh[2][2];          // alpha (CTA 0 only), by parity
-  __shared__ double red_w[2][2 * NB];        // CTA partials of the NB-1 inner products, by parity
-  __shared__ double wsum[QR_NT / 32][2 * NB];
-  __shared__ dcplx wfin[NB];
+  constexpr int NV = 2 * NB;       // reduction slots: [0] ||x||^2, [1 + 2s, 2 + 2s] complex slot s
+  constexpr int SPL = 32 / NV;     // lanes per slot after the reduce-scatter
+  extern __shared__ dcplx xs[];    // xs[(k NB + j) QR_NT + tid]
+  __shared__ double wsum[QR_NT / 32][NV];
+  __shared__ double red[2][QR_CL][NV];   // partials pushed by every CTA of the cluster
+  __shared__ double rowc[2][2 * NB];     // row c of the panel, pushed by CTA 0
+  __shared__ double fin[NV + 2 * NB];
   __shared__ dcplx Tsh[NB][NB + 1];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint32_t rank = cluster_rank();
   const int g = (int)rank * QR_NT + tid;
+#define XS(k, j) xs[((k) * NB + (j)) * QR_NT + tid]
 
-  dcplx x[RPT][NB];
 #pragma unroll
   for (int k = 0; k < RPT; ++k) {
     const int il = g + k * QR_G;
 #pragma unroll
-    for (int j = 0; j < NB; ++j)
-      x[k][j] = (il < R && j < b) ? A[il + lda * (int64_t)j] : make_double2(0.0, 0.0);
+    for (int j = 0; j < NB; ++j) XS(k, j) = (il < R && j < b) ? A[il + lda * (int64_t)j] : make_double2(0.0, 0.0);
   }
   if (rank == 0)
     for (int e = tid; e < NB * (NB + 1); e += QR_NT) Tsh[e / (NB + 1)][e % (NB + 1)] = make_double2(0.0, 0.0);
 
   for (int c = 0; c < b; ++c) {
     const int par = c & 1;
-    // (a) ||x_below||^2 over the rows below the diagonal; alpha = row c (CTA 0, thread c)
-    double ssq = 0.0;
+    double val[NV];
+#pragma unroll
+    for (int s = 0; s < NV; ++s) val[s] = 0.0;
 #pragma unroll
     for (int k = 0; k < RPT; ++k) {
       const int il = g + k * QR_G;
+      if (il > c && il < R) {
+        const dcplx xc = XS(k, c);
+        val[0] = fma(xc.x, xc.x, fma(xc.y, xc.y, val[0]));
 #pragma unroll
-      for (int j = 0; j < NB; ++j)
-        if (j == c && il > c && il < R) ssq = fma(x[k][j].x, x[k][j].x, fma(x[k][j].y, x[k][j].y, ssq));
-    }
-    if (g == c) {
-#pragma unroll
-      for (int j = 0; j < NB; ++j)
-        if (j == c) {
-          alpha_sh[par][0] = x[0][j].x;
-          alpha_sh[par][1] = x[0][j].y;
+        for (int s = 0; s < NB - 1; ++s) {
+          dcplx p = make_double2(0.0, 0.0);
+          if (s < c) p = cmulc(XS(k, s), xc);                // e_s
+          else if (s + 1 < b) p = cmulc(xc, XS(k, s + 1));   // d_{s+1}
+          val[1 + 2 * s] += p.x;
+          val[2 + 2 * s] += p.y;
         }
+      }
     }
-    for (int o = 16; o > 0; o >>= 1) ssq += __shfl_down_sync(0xffffffffu, ssq, o);
-    if (lane == 0) wsum[warp][0] = ssq;
+    const double wv = warp_reduce_scatter<NV>(val, lane);
+    if (lane % SPL == 0) wsum[warp][lane / SPL] = wv;
     __syncthreads();
-    if (tid == 0) {
-      double s = 0.0;
-      for (int q = 0; q < QR_NT / 32; ++q) s += wsum[q][0];
-      red_ssq[par] = s;
+    // push this CTA's partials (and, from CTA 0, row c of the panel: thread c's row
+    // in shared memory) into every CTA of the cluster; no remote loads
+    if (tid < NV) {
+      double t = 0.0;
+      for (int q = 0; q < QR_NT / 32; ++q) t += wsum[q][tid];
+#pragma unroll
+      for (uint32_t q = 0; q < QR_CL; ++q) st_peer(&red[par][rank][tid], q, t);
+    } else if (rank == 0 && tid < NV + 2 * NB * QR_CL) {
+      const int e = tid - NV, slot = e % (2 * NB), dst = e / (2 * NB);
+      const dcplx x = xs[(slot >> 1) * QR_NT + c];   // XS(0, slot / 2) of thread c
+      st_peer(&rowc[par][slot], (uint32_t)dst, (slot & 1) ? x.y : x.x);
     }
     cluster_sync();
-    // (b) the reflector, computed identically by every thread of the cluster
-    double xs = 0.0;
-    for (uint32_t q = 0; q < QR_CL; ++q) xs += ld_peer(&red_ssq[par], q);
-    const dcplx al = make_double2(ld_peer(&alpha_sh[par][0], 0), ld_peer(&alpha_sh[par][1], 0));
+    if (tid < NV) {
+      double t = 0.0;
+#pragma unroll
+      for (int q = 0; q < QR_CL; ++q) t += red[par][q][tid];
+      fin[tid] = t;
+    } else if (tid < NV + 2 * NB) {
+      fin[tid] = rowc[par][tid - NV];
+    }
+    __syncthreads();
+    // the reflector (LAPACK zlarfg), computed identically by every thread
+    const double xsq = fin[0];
+    const dcplx al = make_double2(fin[NV + 2 * c], fin[NV + 2 * c + 1]);
     dcplx tc, scale;
     double beta;
-    if (xs == 0.0 && al.y == 0.0) {
+    if (xsq == 0.0 && al.y == 0.0) {
       tc = make_double2(0.0, 0.0);
       scale = make_double2(0.0, 0.0);
       beta = al.x;
     } else {
-      beta = -copysign(sqrt(al.x * al.x + al.y * al.y + xs), al.x);
+      beta = -copysign(sqrt(al.x * al.x + al.y * al.y + xsq), al.x);
       tc = make_double2((beta - al.x) / beta, -al.y / beta);
-      // 1 / (alpha - beta)
       const double dr = al.x - beta, di = al.y, den = dr * dr + di * di;
-      scale = make_double2(dr / den, -di / den);
+      scale = make_double2(dr / den, -di / den);   // 1 / (alpha - beta)
     }
-    // (c) v (kept in vk), R diagonal; inner products of v with V[:, 0:c] (for T) and
-    // with the trailing panel columns (for their update), slot s <-> column s < c ? s : s+1
-    dcplx vk[RPT];
-    double acc[2 * NB];
-#pragma unroll
-    for (int s = 0; s < 2 * NB; ++s) acc[s] = 0.0;
+    const dcplx ctc = make_double2(tc.x, -tc.y), cs = make_double2(scale.x, -scale.y);
+    // v into column c, R diagonal, trailing panel columns x_j -= conj(tau) v (v^H x_j)
 #pragma unroll
     for (int k = 0; k < RPT; ++k) {
       const int il = g + k * QR_G;
-      dcplx v = make_double2(0.0, 0.0);
-#pragma unroll
-      for (int j = 0; j < NB; ++j) {
-        if (j == c && il < R) {
-          if (il > c) {
-            v = cmul(x[k][j], scale);
-            x[k][j] = v;
-          } else if (il == c) {
-            v = make_double2(1.0, 0.0);
-            x[k][j] = make_double2(beta, 0.0);
-          }
-        }
+      if (il < c || il >= R) continue;
+      dcplx v;
+      if (il == c) {
+        v = make_double2(1.0, 0.0);
+        XS(k, c) = make_double2(beta, 0.0);
+      } else {
+        v = cmul(XS(k, c), scale);
+        XS(k, c) = v;
       }
-      vk[k] = v;
-#pragma unroll
-      for (int j = 0; j < NB - 1; ++j) {
-        if (j < c) {
-          // V[il, j] = x (il > j), 1 (il == j), 0 above
-          const dcplx vj = il > j ? x[k][j] : (il == j ? make_double2(1.0, 0.0) : make_double2(0.0, 0.0));
-          const dcplx p = cmulc(vj, v);
-          acc[2 * j] += p.x;
-          acc[2 * j + 1] += p.y;
-        } else if (j + 1 < b) {
-          const dcplx p = cmulc(v, x[k][j + 1]);
-          acc[2 * j] += p.x;
-          acc[2 * j + 1] += p.y;
-        }
-      }
-    }
-#pragma unroll
-    for (int s = 0; s < 2 * (NB - 1); ++s) {
-      double t = acc[s];
-      for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
-      if (lane == 0) wsum[warp][s] = t;
-    }
-    __syncthreads();
-    if (tid < 2 * (NB - 1)) {
-      double s = 0.0;
-      for (int q = 0; q < QR_NT / 32; ++q) s += wsum[q][tid];
-      red_w[par][tid] = s;
-    }
-    cluster_sync();
-    if (tid < NB - 1) {
-      double sr = 0.0, si = 0.0;
-      for (uint32_t q = 0; q < QR_CL; ++q) {
-        sr += ld_peer(&red_w[par][2 * tid], q);
-        si += ld_peer(&red_w[par][2 * tid + 1], q);
-      }
-      wfin[tid] = make_double2(sr, si);
-    }
-    __syncthreads();
-    // (d) trailing panel columns: x[:, c'] -= conj(tau) v w_{c'}
-    const dcplx ctc = make_double2(tc.x, -tc.y);
-#pragma unroll
-    for (int k = 0; k < RPT; ++k) {
-      const dcplx cv = cmul(ctc, vk[k]);
+      const dcplx cv = cmul(ctc, v);
 #pragma unroll
       for (int j = 1; j < NB; ++j) {
         if (j > c && j < b) {
-          const dcplx p = cmul(cv, wfin[j - 1]);
-          x[k][j].x -= p.x;
-          x[k][j].y -= p.y;
+          const dcplx dj = make_double2(fin[1 + 2 * (j - 1)], fin[2 + 2 * (j - 1)]);
+          const dcplx rj = make_double2(fin[NV + 2 * j], fin[NV + 2 * j + 1]);
+          const dcplx t = cmul(cs, dj);
+          const dcplx w = make_double2(rj.x + t.x, rj.y + t.y);
+          const dcplx p = cmul(cv, w);
+          dcplx x = XS(k, j);
+          x.x -= p.x;
+          x.y -= p.y;
+          XS(k, j) = x;
         }
       }
     }
-    // (e) T[0:c, c] = -tau_c T[0:c, 0:c] z with z_l = <V_l, v_c> (slots l < c)
+    // T[0:c, c] = -tau T[0:c, 0:c] z with z_l = V_l^H v = conj(V_l[c]) + scale e_l (LAPACK zlarft)
     if (rank == 0) {
       if (tid < c) {
-        dcplx s = make_double2(0.0, 0.0);
+        dcplx sacc = make_double2(0.0, 0.0);
         for (int l = tid; l < c; ++l) {
-          const dcplx p = cmul(Tsh[tid][l], wfin[l]);
-          s.x += p.x;
-          s.y += p.y;
+          const dcplx el = make_double2(fin[1 + 2 * l], fin[2 + 2 * l]);
+          const dcplx se = cmul(scale, el);
+          const dcplx z = make_double2(fin[NV + 2 * l] + se.x, -fin[NV + 2 * l + 1] + se.y);
+          const dcplx p = cmul(Tsh[tid][l], z);
+          sacc.x += p.x;
+          sacc.y += p.y;
         }
-        const dcplx t = cmul(tc, s);
+        const dcplx t = cmul(tc, sacc);
         Tsh[tid][c] = make_double2(-t.x, -t.y);
       }
       if (tid == 0) {
@@ -240,11 +250,15 @@ __global__ void __cluster_dims__(QR_CL, 1, 1) __launch_bounds__(QR_NT, 1)
 #pragma unroll
     for (int j = 0; j < NB; ++j) {
       if (j < b) {
-        A[il + lda * (int64_t)j] = x[k][j];
-        V[il + ldv * (int64_t)j] = il > j ? x[k][j] : (il == j ? make_double2(1.0, 0.0) : make_double2(0.0, 0.0));
+        const dcplx x = XS(k, j);
+        A[il + lda * (int64_t)j] = x;
+        V[il + ldv * (int64_t)j] = il > j ? x : (il == j ? make_double2(1.0, 0.0) : make_double2(0.0, 0.0));
       }
     }
   }
+#undef XS
+  for (int r = g; r < zabove; r += QR_G)
+    for (int j = 0; j < b; ++j) V[(int64_t)(r - zabove) + ldv * (int64_t)j] = make_double2(0.0, 0.0);
   if (rank == 0) {
     __syncthreads();
     for (int e = tid; e < b * b; e += QR_NT) {
@@ -254,6 +268,57 @@ __global__ void __cluster_dims__(QR_CL, 1, 1) __launch_bounds__(QR_NT, 1)
   }
   // no CTA may leave while a peer can still read its shared memory
   cluster_sync();
+}
+
+// Compact-WY factor of an outer block from the factors of its inner panels (LAPACK
+// zlarft, block form): T = [[T1, -T1 (V1^H V2) T2], [0, T2]] applied panel by panel,
+// with G = V^H V of the whole outer block.  One CTA; T is bo x bo (ld bo).
+struct PanelList {
+  int n;
+  short off[QR_NBO / 2 + 1];
+  short w[QR_NBO / 2];
+};
+
+__global__ void __launch_bounds__(256) k_merge_t(int bo, PanelList pl, const dcplx* __restrict__ Tin,
+                                                 const dcplx* __restrict__ G, dcplx* __restrict__ Tb) {
+  __shared__ dcplx Xs[QR_NBO][QR_NBMAX];
+  const int tid = threadIdx.x;
+  for (int e = tid; e < bo * bo; e += blockDim.x) {
+    const int r = e % bo, c = e / bo;
+    int t = 0;
+    while (t + 1 < pl.n && pl.off[t + 1] <= c) ++t;
+    const int o = pl.off[t];
+    dcplx v = make_double2(0.0, 0.0);
+    if (r >= o && r < o + pl.w[t]) v = Tin[(size_t)t * QR_NBMAX * QR_NBMAX + (r - o) + QR_NBMAX * (c - o)];
+    Tb[r + (int64_t)bo * c] = v;
+  }
+  __syncthreads();
+  for (int t = 1; t < pl.n; ++t) {
+    const int c0 = pl.off[t], bt = pl.w[t];
+    const dcplx* Tt = Tin + (size_t)t * QR_NBMAX * QR_NBMAX;
+    for (int e = tid; e < c0 * bt; e += blockDim.x) {
+      const int r = e % c0, u = e / c0;
+      dcplx s = make_double2(0.0, 0.0);
+      for (int l = r; l < c0; ++l) {
+        const dcplx p = cmul(Tb[r + (int64_t)bo * l], G[l + (int64_t)bo * (c0 + u)]);
+        s.x += p.x;
+        s.y += p.y;
+      }
+      Xs[r][u] = s;
+    }
+    __syncthreads();
+    for (int e = tid; e < c0 * bt; e += blockDim.x) {
+      const int r = e % c0, u = e / c0;
+      dcplx s = make_double2(0.0, 0.0);
+      for (int v = 0; v <= u; ++v) {
+        const dcplx p = cmul(Xs[r][v], Tt[v + QR_NBMAX * u]);
+        s.x += p.x;
+        s.y += p.y;
+      }
+      Tb[r + (int64_t)bo * (c0 + u)] = make_double2(-s.x, -s.y);
+    }
+    __syncthreads();
+  }
 }
 
 __global__ void k_extract_r(int k, int n, const dcplx* __restrict__ A, int64_t lda, dcplx* __restrict__ R,
@@ -285,9 +350,16 @@ __global__ void k_sum_partials(int64_t len, int nc, const dcplx* __restrict__ pa
 }
 
 template <int NB, int RPT>
-void launch_panel(Context* ctx, int R, int b, dcplx* A, int64_t lda, dcplx* V, int64_t ldv, dcplx* tau, dcplx* T,
-                  int ldt) {
-  k_qr_panel<NB, RPT><<<QR_CL, QR_NT, 0, ctx->stream>>>(R, b, A, lda, V, ldv, tau, T, ldt);
+void launch_panel(Context* ctx, int R, int b, int zabove, dcplx* A, int64_t lda, dcplx* V, int64_t ldv, dcplx* tau,
+                  dcplx* T, int ldt) {
+  static_assert(NB * RPT == QR_NBMAX, "panel shared-memory size");
+  static bool attr = false;  // set once per process (one device type)
+  if (!attr) {
+    IMPS_CUDA(cudaFuncSetAttribute(k_qr_panel<NB, RPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)QR_PANEL_SMEM));
+    attr = true;
+  }
+  k_qr_panel<NB, RPT><<<QR_CL, QR_NT, QR_PANEL_SMEM, ctx->stream>>>(R, b, zabove, A, lda, V, ldv, tau, T, ldt);
   ctx->n_kernels++;
   cudaError_t e = cudaPeekAtLastError();
   if (e != cudaSuccess) throw Error(IMPS_CUDA_ERROR, std::string("qr panel launch: ") + cudaGetErrorString(e));
@@ -301,26 +373,39 @@ int panel_width(int R) {
   return 2;
 }
 
-// W (b x N) = V^H X with V (K x b) and X (K x N) sharing the leading dimension ld and a
-// long K: split into chunks of QR_KC rows (one batched GEMM over the full chunks and
-// one for the remainder), then a deterministic sum of the partial products.
-void gemm_vhx(Context* ctx, int b, int N, int K, const dcplx* Vm, const dcplx* X, int64_t ld, dcplx* part,
-              dcplx* W) {
-  const int nfull = K / QR_KC, rem = K - nfull * QR_KC;
-  const int nc = nfull + (rem > 0 ? 1 : 0);
-  const int64_t pstride = (int64_t)b * N;
+// Wh (N x b, ld N) = X^H V with X (K x N) and V (K x b) sharing the leading dimension ld
+// and a long K.  The long side N goes on the GEMM's 128-row output tile; K is split into
+// row chunks (one batched GEMM over the full chunks and one for the remainder) so that
+// about two CTAs per SM are busy, then the partial products are summed in a fixed order.
+void gemm_xhv(Context* ctx, int N, int b, int K, const dcplx* X, const dcplx* Vm, int64_t ld, dcplx* part,
+              dcplx* Wh) {
+  const int tiles = ((N + 127) / 128) * ((b + 63) / 64);
+  int nc = std::max(1, std::min({(2 * 148 + tiles - 1) / tiles, QR_MAXCHUNK, K / 64}));
+  int kc = (K + nc - 1) / nc;
+  kc = (kc + 15) / 16 * 16;
+  nc = (K + kc - 1) / kc;
   if (nc == 1) {
-    zgemm_fp64(ctx, OP_C, OP_N, b, N, K, 1.0, Vm, ld, 0, X, ld, 0, 0.0, W, b, 0, 1);
+    zgemm_fp64(ctx, OP_C, OP_N, N, b, K, 1.0, X, ld, 0, Vm, ld, 0, 0.0, Wh, N, 0, 1);
     return;
   }
+  const int nfull = K / kc, rem = K - nfull * kc;
+  const int64_t pstride = (int64_t)N * b;
   if (nfull > 0)
-    zgemm_fp64(ctx, OP_C, OP_N, b, N, QR_KC, 1.0, Vm, ld, QR_KC, X, ld, QR_KC, 0.0, part, b, pstride, nfull);
+    zgemm_fp64(ctx, OP_C, OP_N, N, b, kc, 1.0, X, ld, kc, Vm, ld, kc, 0.0, part, N, pstride, nfull);
   if (rem > 0)
-    zgemm_fp64(ctx, OP_C, OP_N, b, N, rem, 1.0, Vm + (int64_t)nfull * QR_KC, ld, 0, X + (int64_t)nfull * QR_KC, ld, 0,
-               0.0, part + pstride * nfull, b, 0, 1);
+    zgemm_fp64(ctx, OP_C, OP_N, N, b, rem, 1.0, X + (int64_t)nfull * kc, ld, 0, Vm + (int64_t)nfull * kc, ld, 0,
+               0.0, part + pstride * nfull, N, 0, 1);
   const int g = (int)std::min<int64_t>((pstride + 255) / 256, 148 * 8);
-  k_sum_partials<<<std::max(g, 1), 256, 0, ctx->stream>>>(pstride, nc, part, pstride, W);
+  k_sum_partials<<<std::max(g, 1), 256, 0, ctx->stream>>>(pstride, nc, part, pstride, Wh);
   ctx->n_kernels++;
+}
+
+// A2 (R x N) <- A2 - Y Wh^H with Y = V op(T) (R x b): one block-reflector application
+// given Wh = A2^H V (op = C: A2 <- (I - V T V^H)^H A2; op = N: A2 <- (I - V T V^H) A2).
+void apply_block(Context* ctx, int R, int N, int b, const dcplx* Vp, int64_t ldv, const dcplx* Tp, int ldt, Op opT,
+                 const dcplx* Wh, dcplx* Y, dcplx* A2, int64_t lda) {
+  zgemm_fp64(ctx, OP_N, opT, R, b, b, 1.0, Vp, ldv, 0, Tp, ldt, 0, 0.0, Y, R, 0, 1);
+  zgemm_fp64(ctx, OP_N, OP_C, R, N, b, -1.0, Y, R, 0, Wh, N, 0, 1.0, A2, lda, 0, 1);
 }
 
 }  // namespace
@@ -333,40 +418,65 @@ void qrpos(Context* ctx, int m, int n, const dcplx* M, int64_t ldm, dcplx* Q, dc
   const double qf = 8.0 * (2.0 * m * (double)n * k - 2.0 / 3.0 * k * (double)k * k) * 2.0;
   ctx->qr_flops += qf;
   ScopedTimer t(ctx, "qr", qf);
-  const int npan_max = (k + 1) / 2;
+  const int nob = (k + QR_NBO - 1) / QR_NBO;
+  const int wmax = std::max({n, k, QR_NBO});
   DevBuf& Ab = ctx->buf("qr_a", (size_t)m * n * sizeof(dcplx));
   DevBuf& Vb = ctx->buf("qr_v", (size_t)m * k * sizeof(dcplx));
-  DevBuf& Tb = ctx->buf("qr_t", (size_t)npan_max * QR_NBMAX * QR_NBMAX * sizeof(dcplx));
+  DevBuf& Tin = ctx->buf("qr_tin", (size_t)(QR_NBO / 2) * QR_NBMAX * QR_NBMAX * sizeof(dcplx));
+  DevBuf& Tbig = ctx->buf("qr_t", (size_t)nob * QR_NBO * QR_NBO * sizeof(dcplx));
+  DevBuf& Gb = ctx->buf("qr_g", (size_t)QR_NBO * QR_NBO * sizeof(dcplx));
   DevBuf& taub = ctx->buf("qr_tau", (size_t)k * sizeof(dcplx));
   DevBuf& ph = ctx->buf("qr_ph", (size_t)k * sizeof(dcplx));
-  DevBuf& Wb = ctx->buf("qr_w", (size_t)QR_NBMAX * std::max(n, k) * sizeof(dcplx));
-  DevBuf& W2b = ctx->buf("qr_w2", (size_t)QR_NBMAX * std::max(n, k) * sizeof(dcplx));
-  DevBuf& Pb = ctx->buf("qr_part", (size_t)QR_NBMAX * std::max(n, k) * ((m + QR_KC - 1) / QR_KC) * sizeof(dcplx));
+  DevBuf& Wb = ctx->buf("qr_w", (size_t)QR_NBO * wmax * sizeof(dcplx));
+  DevBuf& Yb = ctx->buf("qr_y", (size_t)QR_NBO * m * sizeof(dcplx));
+  DevBuf& Pb = ctx->buf("qr_part", (size_t)QR_NBO * wmax * QR_MAXCHUNK * sizeof(dcplx));
   zcopy2d(ctx, m, n, M, ldm, Ab.z(), m);
   dcplx* A = Ab.z();
-  std::vector<std::pair<int, int>> panels;  // (p, b)
-  for (int p = 0; p < k;) {
-    const int Rr = m - p;
-    const int b = std::min(panel_width(Rr), k - p);
-    dcplx* Ap = A + p + (int64_t)m * p;
-    dcplx* Vp = Vb.z() + p + (int64_t)m * p;
-    dcplx* Tp = Tb.z() + (size_t)panels.size() * QR_NBMAX * QR_NBMAX;
-    switch (panel_width(Rr)) {
-      case 16: launch_panel<16, 1>(ctx, Rr, b, Ap, m, Vp, m, taub.z() + p, Tp, QR_NBMAX); break;
-      case 8: launch_panel<8, 2>(ctx, Rr, b, Ap, m, Vp, m, taub.z() + p, Tp, QR_NBMAX); break;
-      case 4: launch_panel<4, 4>(ctx, Rr, b, Ap, m, Vp, m, taub.z() + p, Tp, QR_NBMAX); break;
-      default: launch_panel<2, 8>(ctx, Rr, b, Ap, m, Vp, m, taub.z() + p, Tp, QR_NBMAX); break;
+  std::vector<std::pair<int, int>> blocks;  // (P, bo)
+  for (int P = 0; P < k;) {
+    const int bo = std::min(QR_NBO, k - P);
+    PanelList pl;
+    pl.n = 0;
+    // inner panels; each also updates the rest of its outer block
+    for (int p = P; p < P + bo;) {
+      const int Rr = m - p;
+      const int b = std::min(panel_width(Rr), P + bo - p);
+      dcplx* Ap = A + p + (int64_t)m * p;
+      dcplx* Vp = Vb.z() + p + (int64_t)m * p;
+      dcplx* Tp = Tin.z() + (size_t)pl.n * QR_NBMAX * QR_NBMAX;
+      switch (panel_width(Rr)) {
+        case 16: launch_panel<16, 1>(ctx, Rr, b, p - P, Ap, m, Vp, m, taub.z() + p, Tp, QR_NBMAX); break;
+        case 8: launch_panel<8, 2>(ctx, Rr, b, p - P, Ap, m, Vp, m, taub.z() + p, Tp, QR_NBMAX); break;
+        case 4: launch_panel<4, 4>(ctx, Rr, b, p - P, Ap, m, Vp, m, taub.z() + p, Tp, QR_NBMAX); break;
+        default: launch_panel<2, 8>(ctx, Rr, b, p - P, Ap, m, Vp, m, taub.z() + p, Tp, QR_NBMAX); break;
+      }
+      pl.off[pl.n] = (short)(p - P);
+      pl.w[pl.n] = (short)b;
+      pl.n++;
+      const int n2in = P + bo - (p + b);
+      if (n2in > 0) {
+        dcplx* A2 = A + p + (int64_t)m * (p + b);
+        gemm_xhv(ctx, n2in, b, Rr, A2, Vp, m, Pb.z(), Wb.z());
+        apply_block(ctx, Rr, n2in, b, Vp, m, Tp, QR_NBMAX, OP_C, Wb.z(), Yb.z(), A2, m);
+      }
+      p += b;
     }
-    const int n2 = n - p - b;
+    pl.off[pl.n] = (short)bo;
+    // compact-WY factor of the outer block, then its trailing update
+    const int RrB = m - P;
+    dcplx* Vblk = Vb.z() + P + (int64_t)m * P;
+    dcplx* Tb = Tbig.z() + (size_t)blocks.size() * QR_NBO * QR_NBO;
+    if (pl.n > 1) gemm_xhv(ctx, bo, bo, RrB, Vblk, Vblk, m, Pb.z(), Gb.z());
+    k_merge_t<<<1, 256, 0, ctx->stream>>>(bo, pl, Tin.z(), Gb.z(), Tb);
+    ctx->n_kernels++;
+    const int n2 = n - (P + bo);
     if (n2 > 0) {
-      dcplx* A2 = A + p + (int64_t)m * (p + b);
-      // W = V^H A2, W2 = T^H W, A2 -= V W2
-      gemm_vhx(ctx, b, n2, Rr, Vp, A2, m, Pb.z(), Wb.z());
-      zgemm_fp64(ctx, OP_C, OP_N, b, n2, b, 1.0, Tp, QR_NBMAX, 0, Wb.z(), b, 0, 0.0, W2b.z(), b, 0, 1);
-      zgemm_fp64(ctx, OP_N, OP_N, Rr, n2, b, -1.0, Vp, m, 0, W2b.z(), b, 0, 1.0, A2, m, 0, 1);
+      dcplx* A2 = A + P + (int64_t)m * (P + bo);
+      gemm_xhv(ctx, n2, bo, RrB, A2, Vblk, m, Pb.z(), Wb.z());
+      apply_block(ctx, RrB, n2, bo, Vblk, m, Tb, bo, OP_C, Wb.z(), Yb.z(), A2, m);
     }
-    panels.push_back({p, b});
-    p += b;
+    blocks.push_back({P, bo});
+    P += bo;
   }
   {
     int64_t tot = (int64_t)k * n;
@@ -374,18 +484,17 @@ void qrpos(Context* ctx, int m, int n, const dcplx* M, int64_t ldm, dcplx* Q, dc
     k_extract_r<<<std::max(g, 1), 256, 0, ctx->stream>>>(k, n, A, m, R, k, ph.z());
     ctx->n_kernels++;
   }
-  // Q = H_1 ... H_k [I; 0], block reflectors applied from the last panel back
+  // Q = H_1 ... H_k [I; 0], outer block reflectors applied from the last block back
   zfill2d(ctx, m, k, 0.0, Q, m);
   zadd_diag(ctx, k, Q, m, 1.0);
-  for (int t = (int)panels.size() - 1; t >= 0; --t) {
-    const int p = panels[t].first, b = panels[t].second;
-    const int Rr = m - p, nc = k - p;
-    dcplx* Vp = Vb.z() + p + (int64_t)m * p;
-    dcplx* Tp = Tb.z() + (size_t)t * QR_NBMAX * QR_NBMAX;
-    dcplx* Qs = Q + p + (int64_t)m * p;
-    gemm_vhx(ctx, b, nc, Rr, Vp, Qs, m, Pb.z(), Wb.z());
-    zgemm_fp64(ctx, OP_N, OP_N, b, nc, b, 1.0, Tp, QR_NBMAX, 0, Wb.z(), b, 0, 0.0, W2b.z(), b, 0, 1);
-    zgemm_fp64(ctx, OP_N, OP_N, Rr, nc, b, -1.0, Vp, m, 0, W2b.z(), b, 0, 1.0, Qs, m, 0, 1);
+  for (int t = (int)blocks.size() - 1; t >= 0; --t) {
+    const int P = blocks[t].first, bo = blocks[t].second;
+    const int RrB = m - P, nc = k - P;
+    dcplx* Vblk = Vb.z() + P + (int64_t)m * P;
+    dcplx* Tb = Tbig.z() + (size_t)t * QR_NBO * QR_NBO;
+    dcplx* Qs = Q + P + (int64_t)m * P;
+    gemm_xhv(ctx, nc, bo, RrB, Qs, Vblk, m, Pb.z(), Wb.z());
+    apply_block(ctx, RrB, nc, bo, Vblk, m, Tb, bo, OP_N, Wb.z(), Yb.z(), Qs, m);
   }
   scale_q_r(ctx, m, n, k, Q, m, R, k, ph.z());
 }

@@ -210,9 +210,10 @@ int svd_thin(Context* ctx, int m, int n, const dcplx* A, int64_t lda, int kmax, 
     s[j] = std::sqrt(std::max(n2[perm[j]], 0.0));
     inv[j] = s[j] > 0.0 ? 1.0 / s[j] : 0.0;
   }
+  // the doubles first: an int array of odd length before them would misalign them
   DevBuf& pb = ctx->buf("svd_perm", (size_t)k * (sizeof(int) + sizeof(double)));
-  int* pd = static_cast<int*>(pb.ptr);
-  double* sd = reinterpret_cast<double*>(static_cast<char*>(pb.ptr) + (size_t)k * sizeof(int));
+  double* sd = static_cast<double*>(pb.ptr);
+  int* pd = reinterpret_cast<int*>(static_cast<char*>(pb.ptr) + (size_t)k * sizeof(double));
   upload(ctx, pd, perm.data(), (size_t)k * sizeof(int));
   upload(ctx, sd, inv.data(), (size_t)k * sizeof(double));
   auto grid = [](int64_t t) { return (int)std::max<int64_t>(1, std::min<int64_t>((t + 255) / 256, 148 * 8)); };

@@ -153,100 +153,100 @@ __global__ void k_proj_update(int64_t n, int nv, const dcplx* __restrict__ V, in
   }
 }
 
-// Block reduction of the per-thread dot accumulators acc[0 .. 2 nv) and the norm
-// accumulator into per-block partials part[blockIdx.x + ldp * k] (k < 2 nv: dots,
-// k = 2 nv: norm), in a fixed order (deterministic).  Indices are compile-time so
-// the accumulators stay in registers.
-template <int NV>
-__device__ __forceinline__ void block_reduce_dots(const double (&acc)[2 * NV], double nrm, int nv, double* part,
-                                                  int64_t ldp) {
-  __shared__ double red[kRedThreads / 32][2 * NV + 1];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-  for (int k = 0; k < 2 * NV; ++k) {
-    if (k < 2 * nv) {
-      double v = acc[k];
-      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-      if (lane == 0) red[wid][k] = v;
-    }
-  }
-  for (int o = 16; o > 0; o >>= 1) nrm += __shfl_down_sync(0xffffffffu, nrm, o);
-  if (lane == 0) red[wid][2 * NV] = nrm;
-  __syncthreads();
-  for (int k = threadIdx.x; k <= 2 * nv; k += blockDim.x) {
-    const int src = k < 2 * nv ? k : 2 * NV;
-    double sum = 0.0;
-    for (int q = 0; q < kRedThreads / 32; ++q) sum += red[q][src];
-    part[blockIdx.x + ldp * k] = sum;
-  }
-}
+// Gram-Schmidt projections against a basis of nv <= NV columns, one kernel per pass.
+// The rows are taken in chunks of GS_ROWS; per chunk the block loads V[chunk, 0:nv]
+// once from HBM (coalesced: 32 consecutive rows per warp and column) into shared
+// memory, optionally applies the pending update w <- w - V h (the column partial sums
+// of each row combined through shared memory), then forms the chunk's contribution
+// to h'_j = <V_j, w> for every column from shared memory, GS_THREADS / NV threads per
+// column.  Few registers per thread: 8 resident blocks of 256 threads per SM keep
+// enough loads in flight for the HBM bandwidth.  Partials: part[blockIdx.x + ldp k],
+// k < 2 nv the dots (re, im interleaved), k = 2 nv the norm^2 of w (after the update).
+constexpr int GS_THREADS = 256;
+constexpr int GS_ROWS = 64;
+constexpr int GS_QP = GS_THREADS / GS_ROWS;
 
-// Gram-Schmidt, first projection: partials of h_j = <V_j, w> (j < nv <= NV,
-// columns 2j, 2j+1) and of ||w||^2 (column 2 nv), one read of V and of w.
-template <int NV>
-__global__ void __launch_bounds__(kRedThreads) k_gs_dots(int64_t n, int nv, const dcplx* __restrict__ V, int64_t ldv,
-                                                     const dcplx* __restrict__ w, double* __restrict__ part,
-                                                     int64_t ldp) {
-  double acc[2 * NV];
-  double nrm = 0.0;
+template <int NV, bool UPDATE>
+__global__ void __launch_bounds__(GS_THREADS) k_gs_pass(int64_t n, int nv, const dcplx* __restrict__ V, int64_t ldv,
+                                                       const double* __restrict__ hdev, dcplx* __restrict__ w,
+                                                       double* __restrict__ part, int64_t ldp) {
+  constexpr int TPC = GS_THREADS / NV;   // threads per column in the dot phase
+  constexpr int RPD = GS_ROWS / TPC;     // rows per thread in the dot phase
+  __shared__ dcplx Vs[NV][GS_ROWS];
+  __shared__ dcplx as[GS_ROWS];
+  __shared__ dcplx apart[UPDATE ? GS_QP : 1][GS_ROWS];
+  __shared__ dcplx cs[NV];
+  __shared__ double nred[GS_THREADS / 32];
+  const int tid = threadIdx.x, lane = tid & 31;
+  if (UPDATE && tid < NV)
+    cs[tid] = tid < nv ? make_double2(-hdev[2 * tid], -hdev[2 * tid + 1]) : make_double2(0.0, 0.0);
+  if (UPDATE) __syncthreads();
+  const int r1 = tid % GS_ROWS, q = tid / GS_ROWS;   // load phase: row r1, columns q + GS_QP u
+  const int jd = tid / TPC, sd = tid % TPC;          // dot phase: column jd, rows sd + TPC u
+  double dre = 0.0, dim = 0.0, nrm = 0.0;
+  for (int64_t base = blockIdx.x * (int64_t)GS_ROWS; base < n; base += (int64_t)gridDim.x * GS_ROWS) {
+    const int64_t i = base + r1;
+    const bool ok = i < n;
+    double ar = 0.0, ai = 0.0;
 #pragma unroll
-  for (int k = 0; k < 2 * NV; ++k) acc[k] = 0.0;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const dcplx wi = w[i];
-#pragma unroll
-    for (int j = 0; j < NV; ++j) {
-      if (j < nv) {
-        const dcplx p = cmulc(V[i + ldv * j], wi);
-        acc[2 * j] += p.x;
-        acc[2 * j + 1] += p.y;
+    for (int u = 0; u < NV / GS_QP; ++u) {
+      const int j = q + GS_QP * u;
+      const dcplx v = (ok && j < nv) ? V[i + ldv * j] : make_double2(0.0, 0.0);
+      Vs[j][r1] = v;
+      if (UPDATE) {
+        const dcplx c = cs[j];
+        ar = fma(c.x, v.x, fma(-c.y, v.y, ar));
+        ai = fma(c.x, v.y, fma(c.y, v.x, ai));
       }
     }
-    nrm = fma(wi.x, wi.x, fma(wi.y, wi.y, nrm));
+    if (UPDATE) {
+      apart[q][r1] = make_double2(ar, ai);
+      __syncthreads();
+      if (tid < GS_ROWS) {
+        dcplx wi = ok ? w[i] : make_double2(0.0, 0.0);
+#pragma unroll
+        for (int t = 0; t < GS_QP; ++t) {
+          wi.x += apart[t][tid].x;
+          wi.y += apart[t][tid].y;
+        }
+        if (ok) w[i] = wi;
+        as[tid] = wi;
+        nrm = fma(wi.x, wi.x, fma(wi.y, wi.y, nrm));
+      }
+    } else if (tid < GS_ROWS) {
+      const dcplx wi = ok ? w[i] : make_double2(0.0, 0.0);
+      as[tid] = wi;
+      nrm = fma(wi.x, wi.x, fma(wi.y, wi.y, nrm));
+    }
+    __syncthreads();
+    if (jd < nv) {
+#pragma unroll
+      for (int u = 0; u < RPD; ++u) {
+        const int r = sd + TPC * u;
+        const dcplx v = Vs[jd][r], a = as[r];
+        dre = fma(v.x, a.x, fma(v.y, a.y, dre));
+        dim = fma(v.x, a.y, fma(-v.y, a.x, dim));
+      }
+    }
+    __syncthreads();
   }
-  block_reduce_dots<NV>(acc, nrm, nv, part, ldp);
-}
-
-// Gram-Schmidt, fused update: w <- w - V h with h = hdev (interleaved re, im), and
-// in the same pass the partials of the next projection's h'_j = <V_j, w_new> and of
-// ||w_new||^2 (same column layout as k_gs_dots).  The second read of V_j for an
-// element follows the first within the same thread and is served from L1/L2, so
-// an iterative-refinement pass costs one HBM read of V instead of two.
-template <int NV>
-__global__ void __launch_bounds__(kRedThreads) k_gs_update_dots(int64_t n, int nv, const dcplx* __restrict__ V,
-                                                            int64_t ldv, const double* __restrict__ hdev,
-                                                            dcplx* __restrict__ w, double* __restrict__ part,
-                                                            int64_t ldp) {
-  __shared__ double2 c[NV];
-  if (threadIdx.x < nv) c[threadIdx.x] = make_double2(-hdev[2 * threadIdx.x], -hdev[2 * threadIdx.x + 1]);
+#pragma unroll
+  for (int o = TPC / 2; o >= 1; o >>= 1) {
+    dre += __shfl_xor_sync(0xffffffffu, dre, o);
+    dim += __shfl_xor_sync(0xffffffffu, dim, o);
+  }
+  if (sd == 0 && jd < nv) {
+    part[blockIdx.x + ldp * (2 * jd)] = dre;
+    part[blockIdx.x + ldp * (2 * jd + 1)] = dim;
+  }
+  for (int o = 16; o > 0; o >>= 1) nrm += __shfl_xor_sync(0xffffffffu, nrm, o);
+  if (lane == 0) nred[tid >> 5] = nrm;
   __syncthreads();
-  double acc[2 * NV];
-  double nrm = 0.0;
-#pragma unroll
-  for (int k = 0; k < 2 * NV; ++k) acc[k] = 0.0;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    dcplx a = w[i];
-#pragma unroll
-    for (int j = 0; j < NV; ++j) {
-      if (j < nv) {
-        const dcplx p = cmul(c[j], V[i + ldv * j]);
-        a.x += p.x;
-        a.y += p.y;
-      }
-    }
-    w[i] = a;
-#pragma unroll
-    for (int j = 0; j < NV; ++j) {
-      if (j < nv) {
-        // a second, separate load (not the register copy of the first): keeps the
-        // live registers to the accumulators
-        const dcplx p = cmulc(__ldca(V + i + ldv * j), a);
-        acc[2 * j] += p.x;
-        acc[2 * j + 1] += p.y;
-      }
-    }
-    nrm = fma(a.x, a.x, fma(a.y, a.y, nrm));
+  if (tid == 0) {
+    double t = 0.0;
+    for (int k = 0; k < GS_THREADS / 32; ++k) t += nred[k];
+    part[blockIdx.x + ldp * (2 * nv)] = t;
   }
-  block_reduce_dots<NV>(acc, nrm, nv, part, ldp);
 }
 
 struct CoefPack {
@@ -600,9 +600,9 @@ template <int NV>
 void launch_gs(Context* ctx, bool update, int nb, int64_t n, int nv, const dcplx* V, int64_t ldv, const double* hdev,
                dcplx* w, double* part) {
   if (update)
-    k_gs_update_dots<NV><<<nb, kRedThreads, 0, ctx->stream>>>(n, nv, V, ldv, hdev, w, part, nb);
+    k_gs_pass<NV, true><<<nb, GS_THREADS, 0, ctx->stream>>>(n, nv, V, ldv, hdev, w, part, nb);
   else
-    k_gs_dots<NV><<<nb, kRedThreads, 0, ctx->stream>>>(n, nv, V, ldv, w, part, nb);
+    k_gs_pass<NV, false><<<nb, GS_THREADS, 0, ctx->stream>>>(n, nv, V, ldv, hdev, w, part, nb);
   check_launch(ctx);
 }
 void gs_pass(Context* ctx, bool update, int nb, int64_t n, int nv, const dcplx* V, int64_t ldv, const double* hdev,
@@ -613,6 +613,8 @@ void gs_pass(Context* ctx, bool update, int nb, int64_t n, int nv, const dcplx* 
   k_final_sum_cols<<<2 * nv + 1, kRedThreads, 0, ctx->stream>>>(nb, part, nb, out);
   check_launch(ctx);
 }
+// blocks of a Gram-Schmidt pass: one chunk per block at most, 8 blocks per SM
+int gs_blocks(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + GS_ROWS - 1) / GS_ROWS, 148 * 8)); }
 const char* kNonFinite =
     "non-finite value (NaN or Inf) in the Krylov iteration: the operator or the start vector holds one";
 }  // namespace
@@ -638,7 +640,7 @@ double gs_project(Context* ctx, int64_t n, int nv, const dcplx* V, int64_t ldv, 
     }
     return std::sqrt(std::max(nw1, 0.0));
   }
-  const int nb = std::min(red_blocks(n), 592);
+  const int nb = gs_blocks(n);
   const int ncol = 2 * nv + 1;
   DevBuf& part = ctx->buf("gs_part", (size_t)nb * ncol * sizeof(double));
   DevBuf& outb = ctx->buf("gs_out", (size_t)3 * ncol * sizeof(double));
