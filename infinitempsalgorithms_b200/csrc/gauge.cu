@@ -79,7 +79,19 @@ GaugeResult uniform_leftorth(Context* ctx, imps_state* st, const std::vector<con
         }
       };
       DevBuf& ev = ctx->buf("gauge_evec", (size_t)DN * DN * sizeof(dcplx));
-      arnoldi_dominant(ctx, (int64_t)DN * DN, op, st->C[N - 1].z(), ev.z(), etol, 30, 300, true);
+      {
+        // the fixed point only seeds the next sweep, whose own FP64 convergence test decides;
+        // its transfer products may run on the split engine at a tenth of the eigensolver
+        // tolerance (the site tensors are constant over the eigensolve: splits cached)
+        std::vector<const void*> cptrs;
+        for (int l = 0; l < N; ++l) {
+          cptrs.push_back(Aw[l]);
+          cptrs.push_back(st->AL[l].ptr);
+        }
+        ConstScope cs(ctx, cptrs);
+        SplitAllowScope sa(ctx, 0.1 * etol);
+        arnoldi_dominant(ctx, (int64_t)DN * DN, op, st->C[N - 1].z(), ev.z(), etol, 30, 300, true);
+      }
       DevBuf& q = ctx->buf("gauge_q", (size_t)DN * DN * sizeof(dcplx));
       qrpos(ctx, DN, DN, ev.z(), DN, q.z(), st->C[N - 1].z());
     }
@@ -138,7 +150,19 @@ GaugeResult uniform_rightorth(Context* ctx, imps_state* st, const std::vector<co
         }
       };
       DevBuf& ev = ctx->buf("gauge_evec", (size_t)DN * DN * sizeof(dcplx));
-      arnoldi_dominant(ctx, (int64_t)DN * DN, op, st->C[N - 1].z(), ev.z(), etol, 30, 300, true);
+      {
+        // the fixed point only seeds the next sweep, whose own FP64 convergence test decides;
+        // its transfer products may run on the split engine at a tenth of the eigensolver
+        // tolerance (the site tensors are constant over the eigensolve: splits cached)
+        std::vector<const void*> cptrs;
+        for (int l = 0; l < N; ++l) {
+          cptrs.push_back(Aw[l]);
+          cptrs.push_back(st->AR[l].ptr);
+        }
+        ConstScope cs(ctx, cptrs);
+        SplitAllowScope sa(ctx, 0.1 * etol);
+        arnoldi_dominant(ctx, (int64_t)DN * DN, op, st->C[N - 1].z(), ev.z(), etol, 30, 300, true);
+      }
       DevBuf& q = ctx->buf("gauge_q", (size_t)DN * DN * sizeof(dcplx));
       lqpos(ctx, DN, DN, ev.z(), DN, st->C[N - 1].z(), q.z());
     }

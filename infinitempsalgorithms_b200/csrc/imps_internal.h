@@ -189,6 +189,29 @@ struct Fp64Scope {
   explicit Fp64Scope(Context* c) : ctx(c) { ctx->force_fp64++; }
   ~Fp64Scope() { ctx->force_fp64--; }
 };
+// Inside an Fp64Scope: lets the split engine serve the GEMMs at accuracy tol while alive,
+// when the context runs the split engine with adaptive slice counts (the slice count then
+// follows tol; a fixed count could not reach an arbitrary tolerance).
+struct SplitAllowScope {
+  Context* ctx;
+  int saved;
+  double old_tol;
+  bool on;
+  SplitAllowScope(Context* c, double tol)
+      : ctx(c), saved(c->force_fp64), old_tol(c->split_tol),
+        on(c->precision == PREC_SPLIT_I8 && c->adaptive_slices) {
+    if (on) {
+      ctx->force_fp64 = 0;
+      ctx->split_tol = tol;
+    }
+  }
+  ~SplitAllowScope() {
+    if (on) {
+      ctx->force_fp64 = saved;
+      ctx->split_tol = old_tol;
+    }
+  }
+};
 // Sets the accuracy the split GEMMs must meet while alive.
 struct TolScope {
   Context* ctx;
