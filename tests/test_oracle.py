@@ -187,6 +187,56 @@ def test_hubbard_model_hermitian_and_anchor():
     W = H[0]
     h2 = sum(np.kron(W[0, :, k, :], W[k, :, 5, :]) for k in range(1, 5))
     assert np.linalg.norm(h2 - h2.conj().T) < 1e-14
-    # two-site ring exact diagonalisation sanity: particle-hole symmetric spectrum at mu = U/2
+    # the Lieb-Wu anchor and the TFIM anchor used by the energy checks
     assert abs(O.hubbard_e0() - (-2.5737293678984)) < 1e-9
     assert abs(O.tfim_e0() + 4 / math.pi) < 1e-12
+
+
+def _open_chain_from_mpo(W, L):
+    """Hamiltonian of an open chain of L sites from a Schur MPO site tensor W (m, d, n, d):
+    first level at the left end, last level at the right end."""
+    m, d = W.shape[0], W.shape[1]
+    X = [np.eye(1, dtype=complex) if k == 0 else None for k in range(m)]
+    for _ in range(L):
+        Y = [None] * m
+        for a in range(m):
+            if X[a] is None:
+                continue
+            for b in range(m):
+                blk = W[a, :, b, :]
+                if np.any(blk):
+                    t = np.kron(X[a], blk)
+                    Y[b] = t if Y[b] is None else Y[b] + t
+        X = Y
+    return X[m - 1]
+
+
+def test_hubbard_mpo_open_chain_exact_diagonalisation():
+    # the w = 6 Jordan-Wigner Hubbard MPO against an independent second-quantised build on an
+    # open chain of 4 sites (8 fermionic modes, 256 states): identical spectra
+    t, U, mu, L = 1.0, 4.0, 2.0, 4
+    Hm = _open_chain_from_mpo(O.hubbard_hamiltonian()[0], L)
+    nm = 2 * L
+    a = np.array([[0, 1], [0, 0]], dtype=complex)     # annihilates the occupied state |1>
+    z = np.diag([1.0, -1.0]).astype(complex)
+    eye = np.eye(2, dtype=complex)
+
+    def mode_op(k):
+        ops = [z] * k + [a] + [eye] * (nm - k - 1)
+        out = ops[0]
+        for o in ops[1:]:
+            out = np.kron(out, o)
+        return out
+    c = [mode_op(k) for k in range(nm)]           # mode 2 i + s: site i, spin s
+    n = [ck.conj().T @ ck for ck in c]
+    Hf = np.zeros((2 ** nm, 2 ** nm), dtype=complex)
+    for i in range(L - 1):
+        for s in range(2):
+            hop = c[2 * i + s].conj().T @ c[2 * (i + 1) + s]
+            Hf += -t * (hop + hop.conj().T)
+    for i in range(L):
+        Hf += U * n[2 * i] @ n[2 * i + 1] - mu * (n[2 * i] + n[2 * i + 1])
+    assert np.linalg.norm(Hm - Hm.conj().T) < 1e-12
+    em = np.linalg.eigvalsh(Hm)
+    ef = np.linalg.eigvalsh(Hf)
+    assert np.max(np.abs(em - ef)) < 1e-10
