@@ -58,7 +58,9 @@ __all__ = [
     "dominant_env", "normalize_envs", "build_envs_dense", "expectationvalue_dense", "apply_local", "correlator",
     "entanglement_spectrum", "renyi_entropy", "entropy",
     "timeevompo", "timeevompo_site", "mpo_ring",
-    "IDMRG2", "ac2_apply", "ac2", "idmrg2_split", "idmrg2_sweep", "idmrg2_groundstate",
+    "IDMRG2", "ac2_apply", "VOMPS", "MultCache", "push_ternary_left", "push_ternary_right", "mult_ac",
+    "mult_c", "env_start_vector", "mixed_fixedpoints", "mult_galerkin", "svdguess_mult_sites", "mult_sweeps",
+    "mult", "ac2", "idmrg2_split", "idmrg2_sweep", "idmrg2_groundstate",
 ]
 
 C128 = np.complex128
@@ -1863,3 +1865,241 @@ def idmrg2_groundstate(psi0: CanonicalIMPS, H: SchurMPO, alg: IDMRG2, envs: Opti
     psi2 = canonical_from_sites([psi.AR[l] for l in range(N)], tol=ag["tol"], maxiter=ag["maxiter"])
     envs2 = build_envs(psi2, H)
     return psi2, envs2, dict(niter=it, converged=converged, losses=losses, itererr=losses[-1], E=E)
+
+
+# --------------------------------------------------------------------------
+# MPO application mult(W, psi, VOMPS(D)): src/algorithms/arithmetics/mult.jl (MultCache
+# :58-197, local maps :226-230 / :294-303 / :705-716, calc_galerkin :586-593, mult :794-806,
+# svdguess_mult :848-870), compression_sweeps!(::VOMPS) (arithmetics/envs.jl:51-93), the
+# lazy SVD guess (arithmetics/compress.jl:161-190) and the ternary pushes
+# (src/transfermatrix.jl:77-107).  W is a dense MPO (list of (wl, u, wr, d) tensors, the
+# DenseIMPO channel: operator.AL = AR = AC = W, operator.C = identity).
+# --------------------------------------------------------------------------
+@dataclass
+class VOMPS:
+    """``VOMPS(; D, tol, maxiter, verbosity, alg_gauge, alg_environments, alg_orth)``
+    (``src/algorithms/algdefs.jl:118-153``)."""
+    D: int = Defaults.D
+    tol: float = Defaults.tol
+    maxiter: int = Defaults.maxiter
+    alg_gauge: object = field(default_factory=alg_gauge)
+    alg_environments: object = field(default_factory=alg_environments)
+
+
+def push_ternary_left(L, below, W, above):
+    """``L'[bl',w',al'] = sum conj(below[bl,u,bl']) L[bl,w,al] W[w,u,w',d] above[al,d,al']``
+    (``transfermatrix.jl:77-82``); ``L`` is ``(below bond, w, above bond)``."""
+    Db, du, Dbr = below.shape
+    Da, dd, Dar = above.shape
+    w, wr = W.shape[0], W.shape[2]
+    T1 = freshape(freshape(L, (Db * w, Da)) @ freshape(above, (Da, dd * Dar)), (Db, w, dd, Dar))
+    T2 = np.asfortranarray(np.einsum("wuvd,bwdc->buvc", W, T1, optimize=True))
+    out = freshape(below, (Db * du, Dbr)).conj().T @ freshape(T2, (Db * du, wr * Dar))
+    return np.asfortranarray(freshape(out, (Dbr, wr, Dar)))
+
+
+def push_ternary_right(R, above, W, below):
+    """``R'[al',w',bl'] = sum above[al',d,al] R[al,w,bl] W[w',u,w,d] conj(below[bl',u,bl])``
+    (``transfermatrix.jl:94-99``); ``R`` is ``(above bond, w, below bond)``."""
+    Dal, dd, Da = above.shape
+    Dbl, du, Db = below.shape
+    wl, w = W.shape[0], W.shape[2]
+    T1 = freshape(freshape(above, (Dal * dd, Da)) @ freshape(R, (Da, w * Db)), (Dal, dd, w, Db))
+    T2 = np.asfortranarray(np.einsum("vuwd,adwb->avub", W, T1, optimize=True))
+    out = freshape(T2, (Dal * wl, du * Db)) @ freshape(below, (Dbl, du * Db)).conj().T
+    return np.asfortranarray(freshape(out, (Dal, wl, Dbl)))
+
+
+def mult_ac(GL, W, GR, x):
+    """``_mapAC`` (``mult.jl:226-230``): ``y[aL,u,aR] = sum GL[aL,w,bL] x[bL,s,bR] W[w,u,w',s]
+    GR[bR,w',aR]`` with ``GL (below, w, above)``, ``GR (above, w', below)``."""
+    Db, w, Da = GL.shape
+    _, d, Dar = x.shape
+    wr, Dbr = W.shape[2], GR.shape[2]
+    T1 = freshape(freshape(GL, (Db * w, Da)) @ freshape(x, (Da, d * Dar)), (Db, w, d, Dar))
+    T2 = np.asfortranarray(np.einsum("wuvs,bwsc->bucv", W, T1, optimize=True))
+    y = freshape(T2, (Db * W.shape[1], Dar * wr)) @ freshape(GR, (Dar * wr, Dbr))
+    return np.asfortranarray(freshape(y, (Db, W.shape[1], Dbr)))
+
+
+def mult_c(GL, GR, C):
+    """``_mapC`` with the identity operator bond weight (``mult.jl:705-716``):
+    ``y[jL,jR] = sum GL[jL,w,w2] C[w2,r2] GR[r2,w,jR]``."""
+    Db, w, Da = GL.shape
+    Dar, _, Dbr = GR.shape
+    U = freshape(C @ freshape(GR, (Dar, w * Dbr)), (Da, w, Dbr))   # U[w2, w, jR]
+    GLp = freshape(np.asfortranarray(GL.transpose(0, 2, 1)), (Db, Da * w))
+    return np.asfortranarray(GLp @ freshape(np.asfortranarray(U), (Da * w, Dbr)))
+
+
+def env_start_vector(n: int) -> np.ndarray:
+    """Deterministic start of the environment eigensolves (the reference draws ``randn``):
+    ``exp(2 pi i frac(k phi))``, ``phi`` the golden ratio conjugate, ``k = 0 .. n-1``."""
+    k = np.arange(n, dtype=np.float64)
+    ph = 2.0 * math.pi * np.mod(k * 0.6180339887498949, 1.0)
+    return np.exp(1j * ph)
+
+
+@dataclass
+class MultCache:
+    """``MultCache`` (``mult.jl:58-66``): ``lefts[l]`` ``(below, w, above)``, ``rights[l]``
+    ``(above, w, below)`` of the ``<below|W|above>`` channel."""
+    Ws: List[np.ndarray]
+    bra: CanonicalIMPS
+    ket: CanonicalIMPS
+    lefts: List[np.ndarray]
+    rights: List[np.ndarray]
+
+
+def mixed_fixedpoints(below: CanonicalIMPS, Ws, above: CanonicalIMPS, tol: float, maxiter: int,
+                      GL0=None, GR0=None, krylovdim: int = Defaults.krylovdim):
+    """``mixed_fixedpoints`` (``mult.jl:93-158``): the :LM fixed points of the ternary transfer
+    matrices, the other sites by pushes, GR Frobenius-normalised, then GL[l+1] divided by
+    ``lambda_l = <below.C[l], mapC(GL[l+1], GR[l], above.C[l])>``."""
+    N = len(below)
+    Lw = len(Ws)
+    Dl = below.AL[0].shape[0]
+    Da = above.AL[0].shape[0]
+    Dw = Ws[0].shape[0]
+
+    def tleft(v):
+        for l in range(N):
+            v = push_ternary_left(v, below.AL[l], Ws[l % Lw], above.AL[l])
+        return v
+
+    def tright(v):
+        for l in range(N - 1, -1, -1):
+            v = push_ternary_right(v, above.AR[l], Ws[l % Lw], below.AR[l])
+        return v
+    v0L = GL0.copy(order="F") if GL0 is not None else freshape(env_start_vector(Dl * Dw * Da), (Dl, Dw, Da))
+    _, vL, _ = arnoldi_dominant(tleft, v0L, tol, krylovdim, maxiter, eager=True)
+    GLs = [None] * N
+    GLs[0] = np.asfortranarray(freshape(np.asarray(vL), (Dl, Dw, Da)))
+    for l in range(1, N):
+        GLs[l] = push_ternary_left(GLs[l - 1], below.AL[l - 1], Ws[(l - 1) % Lw], above.AL[l - 1])
+    v0R = GR0.copy(order="F") if GR0 is not None else freshape(env_start_vector(Da * Dw * Dl), (Da, Dw, Dl))
+    _, vR, _ = arnoldi_dominant(tright, v0R, tol, krylovdim, maxiter, eager=True)
+    GRs = [None] * N
+    GRs[N - 1] = np.asfortranarray(freshape(np.asarray(vR), (Da, Dw, Dl)))
+    for l in range(N - 2, -1, -1):
+        GRs[l] = push_ternary_right(GRs[l + 1], above.AR[l + 1], Ws[(l + 1) % Lw], below.AR[l + 1])
+    GRs = [g / _fnorm(g) for g in GRs]
+    for l in range(N):
+        nx = (l + 1) % N
+        lam = np.vdot(below.C[l], mult_c(GLs[nx], GRs[l], above.C[l]))
+        if lam == 0:
+            raise ValueError(f"ternary environment: local overlap lambda = 0 at site {l + 1}")
+        GLs[nx] = np.asfortranarray(GLs[nx] / lam)
+    return GLs, GRs
+
+
+def mult_local_ac(envs: MultCache, l: int):
+    return mult_ac(envs.lefts[l], envs.Ws[l % len(envs.Ws)], envs.rights[l], envs.ket.AC[l])
+
+
+def mult_local_c(envs: MultCache, l: int):
+    N = len(envs.bra)
+    return mult_c(envs.lefts[(l + 1) % N], envs.rights[l], envs.ket.C[l])
+
+
+def mult_galerkin(envs: MultCache, x: CanonicalIMPS) -> float:
+    """``calc_galerkin(envs::MultCache, x)`` (``mult.jl:586-593``) with ``_galerkin``
+    (``mult.jl:278-284``)."""
+    eps = 0.0
+    for l in range(len(x)):
+        ac = mult_local_ac(envs, l)
+        ac = ac / _fnorm(ac)
+        AL = x.AL[l]
+        Dl, d, Dr = AL.shape
+        A2 = freshape(AL, (Dl * d, Dr))
+        x2 = freshape(ac, (Dl * d, Dr))
+        eps = max(eps, _fnorm(x2 - A2 @ (A2.conj().T @ x2)))
+    return eps
+
+
+def _tsvd_rows(B: np.ndarray, D: int):
+    """``tsvd(B, (1,), (2, 3); trunc = truncdim(D))``: ``B = u diag(s) v``, ``v`` (k, d2, d3)."""
+    r, d2, d3 = B.shape
+    U, S, Vh = np.linalg.svd(freshape(B, (r, d2 * d3)), full_matrices=False)
+    k = min(D, len(S))
+    return U[:, :k], S[:k], np.asfortranarray(freshape(Vh[:k, :], (k, d2, d3)))
+
+
+def svdguess_mult_sites(Ws: Sequence[np.ndarray], ALs: Sequence[np.ndarray], D: int) -> List[np.ndarray]:
+    """``svdguess_mult(Ws, ALs, D)`` (``mult.jl:853-870``) through ``_lazy_svd_guess``
+    (``compress.jl:161-190``): the product's site tensors
+    ``B[(wl, bl), u, (wr, br)] = sum_d W[wl,u,wr,d] AL[bl,d,br]`` (``operators/linalg.jl:15-20``)
+    built right to left with the carry absorbed, each truncated to bond ``D``."""
+    N = len(ALs)
+    Lw = len(Ws)
+
+    def site(i, carry):
+        W4 = Ws[i % Lw]
+        A = ALs[i]
+        wl, u, wr, dd = W4.shape
+        bl, _, br = A.shape
+        if carry is None:
+            B5 = np.einsum("wurd,bdc->wburc", W4, A, optimize=True)
+            return np.asfortranarray(freshape(np.asfortranarray(B5), (wl * bl, u, wr * br)))
+        f = carry.shape[1]
+        l4 = freshape(carry, (wr, br, f))
+        Tb = np.einsum("bdc,rcf->bdrf", A, l4, optimize=True)
+        B3 = np.einsum("wurd,bdrf->wbuf", W4, Tb, optimize=True)
+        return np.asfortranarray(freshape(np.asfortranarray(B3), (wl * bl, u, f)))
+
+    out = [None] * N
+    B = site(N - 1, None)
+    carry = None
+    for i in range(N - 1, 0, -1):
+        u, s, v = _tsvd_rows(B, D)
+        out[i] = v
+        carry = np.asfortranarray(u * s)
+        B = site(i - 1, carry)
+    u, s, v = _tsvd_rows(B, D)
+    out[0] = np.asfortranarray(s[:, None, None] * v)
+    if N >= 2:
+        out[N - 1] = np.asfortranarray(np.einsum("asb,bc->asc", out[N - 1], u, optimize=True))
+    else:
+        r1, s1, r2 = out[0].shape
+        U2, S2, _ = np.linalg.svd(freshape(out[0], (r1 * s1, r2)), full_matrices=False)
+        k2 = min(D, len(S2))
+        out[0] = np.asfortranarray(freshape(U2[:, :k2] * S2[:k2], (r1, s1, k2)))
+    return out
+
+
+def mult_sweeps(envs: MultCache, alg: VOMPS):
+    """``compression_sweeps!(envs::MultCache, alg::VOMPS)`` (``arithmetics/envs.jl:51-93``)."""
+    x = envs.bra
+    N = len(x)
+    eps = mult_galerkin(envs, x)
+    losses = [eps]
+    converged = False
+    it = 0
+    for it in range(1, alg.maxiter + 1):
+        ALs = [regauge(mult_local_ac(envs, l), mult_local_c(envs, l)) for l in range(N)]
+        ag = updatetol(alg.alg_gauge, it - 1, eps)
+        x = canonical_from_AL_keepAL(ALs, x.C[N - 1], ag["tol"], ag["maxiter"])
+        ae = updatetol(alg.alg_environments, it - 1, eps)
+        GLs, GRs = mixed_fixedpoints(x, envs.Ws, envs.ket, ae["tol"], ae["maxiter"],
+                                     GL0=envs.lefts[0], GR0=envs.rights[N - 1])
+        envs = MultCache(envs.Ws, x, envs.ket, GLs, GRs)
+        eps = mult_galerkin(envs, x)
+        losses.append(eps)
+        if eps <= alg.tol:
+            converged = True
+            break
+    return envs, dict(niter=it, converged=converged, losses=losses, itererr=losses[-1])
+
+
+def mult(Ws: Sequence[np.ndarray], psi: CanonicalIMPS, alg: VOMPS):
+    """``mult(W, psi, ::VOMPS)`` (``mult.jl:794-806``) for a dense MPO ``W``: initial state
+    ``svdguess_mult(W, psi, alg.D)``, ternary environments at the initial ``alg_environments``
+    tolerance, then ``compression_sweeps!``.  Returns ``(y, envs, info)``."""
+    if len(psi) % len(Ws) != 0:
+        raise ValueError("incompatible unit-cell lengths of MPS and MPO")
+    x0 = canonical_from_sites(svdguess_mult_sites(Ws, psi.AL, alg.D))
+    ae = alg.alg_environments
+    base = ae.alg if isinstance(ae, DynamicTol) else ae
+    GLs, GRs = mixed_fixedpoints(x0, list(Ws), psi, base["tol"], base["maxiter"])
+    envs, info = mult_sweeps(MultCache(list(Ws), x0, psi, GLs, GRs), alg)
+    return envs.bra, envs, info
