@@ -53,6 +53,7 @@ typedef struct imps_ctx imps_ctx;
 typedef struct imps_mpo imps_mpo;
 typedef struct imps_state imps_state;
 typedef struct imps_envs imps_envs;
+typedef struct imps_mult_envs imps_mult_envs;
 
 /* KrylovKit `ConvergenceInfo` equivalent (converged, numiter, numops, normres). */
 typedef struct {
@@ -368,6 +369,37 @@ int imps_idmrg2_sweep(imps_envs* envs, const imps_mpo* mpo, imps_state* st, int 
 int imps_ac2_apply(imps_envs* envs, const imps_mpo* mpo, int p, const double* x, double* y);
 /* chi[l] = bond dimension right of site l, l = 0..N-1 (bonddim(psi, l+1)). */
 int imps_state_bonds(const imps_state* st, int* chi);
+
+/* ---- MPO application mult(W, psi, VOMPS(D)) (src/algorithms/arithmetics/mult.jl) ----
+ * W is any imps_mpo used as a dense MPO (the DenseIMPO channel: AL = AR = AC = W, C = I).
+ *
+ * svdguess_mult(W, psi, D) then CanonicalIMPS(...) (mult.jl:848-870, compress.jl:161-190):
+ * the product's site tensors streamed right to left from psi.AL with every bond truncated to
+ * D (truncdim), gauge-fixed with (tol, maxiter).  Writes a new state to *out (release it with
+ * imps_state_destroy); its bond dimensions come from imps_state_bonds. */
+int imps_mult_guess(const imps_mpo* W, const imps_state* psi, int D, double tol, int maxiter, imps_state** out,
+                    imps_gauge_info* info);
+/* MultCache(bra, W, ket) (mult.jl:93-197): the :LM fixed points of the <bra|W|ket>
+ * transfer matrices (Arnoldi, krylovdim 30, eager, from a deterministic start vector in place
+ * of the reference's randn), the other sites by ternary pushes (transfermatrix.jl:77-107),
+ * every GR at unit norm and GL[l+1] scaled so that <bra.C[l], mapC(l)> = 1.  bra, W and ket
+ * are borrowed and must outlive the object; sweeps change bra in place. */
+int imps_mult_envs_create(imps_state* bra, const imps_mpo* W, const imps_state* ket, double tol, int maxiter,
+                          imps_mult_envs** out, imps_krylov_info* info);
+int imps_mult_envs_destroy(imps_mult_envs* envs);
+/* lefts[site] (side 0, (bra bond, w, ket bond)) or rights[site] (side 1, (ket bond, w,
+ * bra bond)) to the host. */
+int imps_mult_envs_get(const imps_mult_envs* envs, int side, int site, double* host);
+/* _local_AC(envs, site) (Dl, d, Dr of the bra, mult.jl:294-297) and _local_C(envs, site)
+ * (bond right of site, mult.jl:299-303) to the host; either pointer may be NULL. */
+int imps_mult_local_maps(imps_mult_envs* envs, int site, double* ac, double* c);
+/* calc_galerkin(envs::MultCache, bra) (mult.jl:586-593). */
+int imps_mult_galerkin(imps_mult_envs* envs, double* eps);
+/* One compression_sweeps! iteration for VOMPS (arithmetics/envs.jl:60-85): local maps and
+ * regauge! for every site, gauge_step! with (gauge_tol, gauge_maxiter), the fixed points
+ * re-solved warm with (env_tol, env_maxiter), then *eps = the new Galerkin residual. */
+int imps_mult_sweep(imps_mult_envs* envs, double gauge_tol, int gauge_maxiter, double env_tol, int env_maxiter,
+                    double* eps);
 
 #ifdef __cplusplus
 }

@@ -146,6 +146,13 @@ _SIGS = {
     "imps_idmrg2_sweep": (I32, [P, P, P, I32, D, I32, I32, I32, DP, DP]),
     "imps_ac2_apply": (I32, [P, P, I32, DP, DP]),
     "imps_state_bonds": (I32, [P, C.POINTER(I32)]),
+    "imps_mult_guess": (I32, [P, P, I32, D, I32, PP, C.POINTER(GaugeInfo)]),
+    "imps_mult_envs_create": (I32, [P, P, P, D, I32, PP, C.POINTER(KrylovInfo)]),
+    "imps_mult_envs_destroy": (I32, [P]),
+    "imps_mult_envs_get": (I32, [P, I32, I32, DP]),
+    "imps_mult_local_maps": (I32, [P, I32, DP, DP]),
+    "imps_mult_galerkin": (I32, [P, DP]),
+    "imps_mult_sweep": (I32, [P, D, I32, D, I32, DP]),
 }
 
 _lib = None

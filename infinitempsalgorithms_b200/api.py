@@ -26,7 +26,7 @@ __all__ = [
     "SparseIMPO", "tfim_hamiltonian", "heisenberg_hamiltonian", "hubbard_hamiltonian", "PeriodicVector",
     "CanonicalIMPS", "randomimps", "random_site_tensors", "DMRGCache", "recalculate", "AC_hamiltonian",
     "C_hamiltonian", "fixedpoint", "integrate", "regauge", "calc_galerkin", "expectationvalue", "VUMPS",
-    "IDMRG", "IDMRG2", "ac2_apply", "TDVP", "IterativeConvergenceInfo", "find_groundstate", "timestep", "time_evolve", "linsolve",
+    "IDMRG", "IDMRG2", "ac2_apply", "VOMPS", "MultCache", "svdguess_mult", "mult", "TDVP", "IterativeConvergenceInfo", "find_groundstate", "timestep", "time_evolve", "linsolve",
     "qrpos", "lqpos", "tsvd", "push_env_left", "push_env_right", "push_mpo_left", "push_mpo_right",
     "energy_gradient_mpo", "energy_gradient_AL", "coupling_gradient", "rrule_energy", "find_groundstate_batch",
     "DenseIMPO", "identityimpo", "timeevompo", "dominant_env", "correlator", "entanglement_spectrum", "renyi_entropy", "entropy",
@@ -960,6 +960,19 @@ class IDMRG2:
 
 
 @dataclass
+class VOMPS:
+    """``VOMPS(; D, tol, maxiter, verbosity, alg_gauge, alg_environments, alg_orth, finalize)``
+    (``src/algorithms/algdefs.jl:118-153``); ``alg_orth`` is QRpos."""
+    D: int = Defaults.D
+    tol: float = Defaults.tol
+    maxiter: int = Defaults.maxiter
+    verbosity: int = Defaults.verbosity
+    alg_gauge: object = field(default_factory=Defaults.alg_gauge)
+    alg_environments: object = field(default_factory=Defaults.alg_environments)
+    finalize: Optional[Callable] = None
+
+
+@dataclass
 class TDVP:
     """``TDVP(; integrator, alg_gauge, verbosity, finalize)``."""
     integrator: dict = field(default_factory=Defaults.alg_expsolve)
@@ -1144,6 +1157,117 @@ def _find_groundstate_idmrg2(psi0, H, alg: IDMRG2, envs=None):
     envs2 = DMRGCache(psi2, H, build=False)
     envs2.build(psi2, H, warm=False)
     return psi2, envs2, IterativeConvergenceInfo(it, converged, losses, losses[-1])
+
+
+class MultCache:
+    """``MultCache(bra, W, ket)`` on the device (``src/algorithms/arithmetics/mult.jl:58-197``):
+    the ``<bra|W|ket>`` channel's fixed-point environments, ``lefts[l]`` ``(bra, w, ket)`` and
+    ``rights[l]`` ``(ket, w, bra)``.  Keeps ``bra``, ``W`` and ``ket`` alive; sweeps change
+    ``bra`` in place."""
+
+    def __init__(self, bra: CanonicalIMPS, W: SparseIMPO, ket: CanonicalIMPS, tol=Defaults.tol,
+                 maxiter=Defaults.maxiter):
+        self.ctx = bra.ctx
+        self.bra, self.W, self.ket = bra, W, ket
+        self.N = len(bra)
+        h = C.c_void_p()
+        info = L.KrylovInfo()
+        check(self.ctx.lib.imps_mult_envs_create(bra.h, W.handle(self.ctx), ket.h, tol, maxiter, C.byref(h),
+                                                 C.byref(info)), self.ctx.h)
+        self.h = h
+        self.info = info
+        self.ctx._adopt(self)
+
+    def _w(self, l):
+        return self.W[(l % len(self.W)) + 1]
+
+    def leftenv(self, l: int) -> np.ndarray:
+        i = (l - 1) % self.N
+        out = np.zeros((self.bra.chi[(i - 1) % self.N], self._w(i).shape[0], self.ket.chi[(i - 1) % self.N]),
+                       complex, order="F")
+        check(self.ctx.lib.imps_mult_envs_get(self.h, 0, i, dptr(out)), self.ctx.h)
+        return out
+
+    def rightenv(self, l: int) -> np.ndarray:
+        i = (l - 1) % self.N
+        out = np.zeros((self.ket.chi[i], self._w(i).shape[2], self.bra.chi[i]), complex, order="F")
+        check(self.ctx.lib.imps_mult_envs_get(self.h, 1, i, dptr(out)), self.ctx.h)
+        return out
+
+    def local_maps(self, l: int):
+        """``(_local_AC(envs, l), _local_C(envs, l))`` (1-based ``l``)."""
+        i = (l - 1) % self.N
+        ac = np.zeros(self.bra._shape(L.IMPS_AC, i), complex, order="F")
+        c = np.zeros(self.bra._shape(L.IMPS_C, i), complex, order="F")
+        check(self.ctx.lib.imps_mult_local_maps(self.h, i, dptr(ac), dptr(c)), self.ctx.h)
+        return ac, c
+
+    def galerkin(self) -> float:
+        e = C.c_double()
+        check(self.ctx.lib.imps_mult_galerkin(self.h, C.byref(e)), self.ctx.h)
+        return e.value
+
+    def _release(self):
+        if getattr(self, "h", None):
+            self.ctx.lib.imps_mult_envs_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self._release()
+        except Exception:
+            pass
+
+
+def svdguess_mult(W: SparseIMPO, psi: CanonicalIMPS, D: int, tol=Defaults.tolgauge,
+                  maxiter=Defaults.maxiter) -> CanonicalIMPS:
+    """``svdguess_mult(W, psi, D)`` (``mult.jl:848-870``): the product ``W psi`` streamed right
+    to left through truncating SVDs (bonds <= ``D``), as a mixed-canonical state."""
+    ctx = psi.ctx
+    h = C.c_void_p()
+    info = L.GaugeInfo()
+    check(ctx.lib.imps_mult_guess(W.handle(ctx), psi.h, int(D), tol, maxiter, C.byref(h), C.byref(info)), ctx.h)
+    out = CanonicalIMPS.__new__(CanonicalIMPS)
+    out.ctx = ctx
+    out.N = len(psi)
+    out.dims = list(psi.dims)
+    out.h = h
+    ctx._adopt(out)
+    _refresh_bonds(out)
+    out.gauge_info = info
+    return out
+
+
+def mult(W: SparseIMPO, psi: CanonicalIMPS, alg: Optional[VOMPS] = None):
+    """``mult(W, psi, ::VOMPS)`` (``mult.jl:794-806``) -> ``(y, envs, info)``: ``y ~ W psi`` at
+    bond dimension ``alg.D``, from ``svdguess_mult`` through ``compression_sweeps!``
+    (``arithmetics/envs.jl:51-93``), converged on the Galerkin residual."""
+    alg = alg or VOMPS()
+    if len(psi) % len(W) != 0:
+        raise L.DimensionMismatch(L.IMPS_DIM_MISMATCH, "incompatible unit-cell lengths of MPS and MPO")
+    y = svdguess_mult(W, psi, alg.D)
+    ae0 = alg.alg_environments.alg if isinstance(alg.alg_environments, DynamicTol) else alg.alg_environments
+    envs = MultCache(y, W, psi, tol=ae0["tol"], maxiter=ae0["maxiter"])
+    eps = envs.galerkin()
+    losses = [eps]
+    converged = False
+    it = 0
+    for it in range(1, alg.maxiter + 1):
+        ag = updatetol(alg.alg_gauge, it - 1, eps)
+        ae = updatetol(alg.alg_environments, it - 1, eps)
+        e = C.c_double()
+        check(psi.ctx.lib.imps_mult_sweep(envs.h, ag["tol"], ag["maxiter"], ae["tol"], ae["maxiter"], C.byref(e)),
+              psi.ctx.h)
+        if alg.finalize is not None:
+            y, envs = alg.finalize(it, y, W, envs)
+        eps = e.value
+        losses.append(eps)
+        if alg.verbosity > 0:
+            _logiter("VOMPS", it, eps)
+        if eps <= alg.tol:
+            converged = True
+            break
+    return y, envs, IterativeConvergenceInfo(it, converged, losses, losses[-1])
 
 
 def _find_groundstate_idmrg(psi0, H, alg: IDMRG, envs=None):

@@ -15,6 +15,7 @@
 #include "imps_internal.h"
 #include "krylov.h"
 #include "mpo.h"
+#include "mult.h"
 #include "observables.h"
 
 struct imps_ctx {
@@ -1118,6 +1119,115 @@ int imps_state_bonds(const imps_state* st, int* chi) {
   if (!st || !chi) return IMPS_INVALID_ARG;
   for (int l = 0; l < st->N; ++l) chi[l] = st->chi[l];
   return IMPS_OK;
+}
+
+int imps_mult_guess(const imps_mpo* W, const imps_state* psi, int D, double tol, int maxiter, imps_state** out,
+                    imps_gauge_info* info) {
+  if (!W || !psi || !out || D <= 0 || maxiter <= 0) return IMPS_INVALID_ARG;
+  *out = nullptr;
+  return guard(psi->ctx, [&] {
+    IMPS_REQUIRE(W->ctx == psi->ctx, IMPS_INVALID_ARG, "MPO and state belong to different contexts");
+    imps::GaugeResult g;
+    *out = imps::mult_guess(psi->ctx, W, psi, D, tol, maxiter, &g);
+    fill_gauge(info, g);
+    return conv_status(g.converged);
+  });
+}
+
+int imps_mult_envs_create(imps_state* bra, const imps_mpo* W, const imps_state* ket, double tol, int maxiter,
+                          imps_mult_envs** out, imps_krylov_info* info) {
+  if (!bra || !W || !ket || !out || maxiter <= 0) return IMPS_INVALID_ARG;
+  *out = nullptr;
+  imps_mult_envs* E = new imps_mult_envs();
+  int r = guard(bra->ctx, [&] {
+    IMPS_REQUIRE(W->ctx == bra->ctx && ket->ctx == bra->ctx, IMPS_INVALID_ARG,
+                 "MPO and states belong to different contexts");
+    IMPS_REQUIRE(bra->N == ket->N && ket->N % W->N == 0, IMPS_DIM_MISMATCH,
+                 "incompatible unit-cell lengths of MPS and MPO");
+    for (int l = 0; l < ket->N; ++l) {
+      const imps::MpoSite& Ws = W->sites[l % W->N];
+      IMPS_REQUIRE(Ws.d == ket->d[l] && bra->d[l] == ket->d[l], IMPS_DIM_MISMATCH,
+                   "MPO physical dimension != state physical dimension");
+      IMPS_REQUIRE(Ws.n == W->sites[(l + 1) % W->N].m, IMPS_DIM_MISMATCH, "MPO bond chain mismatch");
+    }
+    E->ctx = bra->ctx;
+    E->device = bra->device;
+    E->N = bra->N;
+    E->W = W;
+    E->bra = bra;
+    E->ket = ket;
+    imps::mult_envs_allocate(E);
+    imps::KrylovResult k = imps::mult_fixedpoints(E->ctx, E, tol, maxiter, false);
+    fill_info(info, k);
+    return conv_status(k.converged);
+  });
+  if (r != IMPS_OK && r != IMPS_NOT_CONVERGED) {
+    delete E;
+    return r;
+  }
+  *out = E;
+  return r;
+}
+
+int imps_mult_envs_destroy(imps_mult_envs* E) {
+  if (!E) return IMPS_OK;
+  cudaSetDevice(E->device);
+  cudaDeviceSynchronize();
+  delete E;
+  return IMPS_OK;
+}
+
+int imps_mult_envs_get(const imps_mult_envs* E, int side, int site, double* host) {
+  if (!E || !host || site < 0 || site >= E->N || (side != 0 && side != 1)) return IMPS_INVALID_ARG;
+  return guard(E->ctx, [&] {
+    const imps::DevBuf& b = side == 0 ? E->lefts[site] : E->rights[site];
+    const imps::MpoSite& Ws = E->W->sites[site % E->W->N];
+    const size_t n = side == 0 ? (size_t)E->bra->Dl(site) * Ws.m * E->ket->Dl(site)
+                               : (size_t)E->ket->Dr(site) * Ws.n * E->bra->Dr(site);
+    imps::download(E->ctx, host, b.ptr, n * sizeof(imps::dcplx));
+    return IMPS_OK;
+  });
+}
+
+int imps_mult_local_maps(imps_mult_envs* E, int site, double* ac, double* c) {
+  if (!E || site < 0 || site >= E->N) return IMPS_INVALID_ARG;
+  return guard(E->ctx, [&] {
+    imps::Context* ctx = E->ctx;
+    imps::Fp64Scope fp64(ctx);
+    const imps_state* bra = E->bra;
+    const imps_state* ket = E->ket;
+    const imps::MpoSite& Ws = E->W->sites[site % E->W->N];
+    if (ac) {
+      imps::DevBuf& y = ctx->buf("abi_mult_ac", bra->site_elems(site) * sizeof(imps::dcplx));
+      imps::mult_ac(ctx, Ws, bra->Dl(site), ket->Dl(site), ket->Dr(site), bra->Dr(site), E->lefts[site].z(),
+                    E->rights[site].z(), ket->AC[site].z(), y.z());
+      imps::download(ctx, ac, y.ptr, bra->site_elems(site) * sizeof(imps::dcplx));
+    }
+    if (c) {
+      imps::DevBuf& y = ctx->buf("abi_mult_c", bra->bond_elems(site) * sizeof(imps::dcplx));
+      imps::mult_c(ctx, Ws.n, bra->Dr(site), ket->Dr(site), bra->Dr(site), E->lefts[(site + 1) % E->N].z(),
+                   E->rights[site].z(), ket->C[site].z(), y.z());
+      imps::download(ctx, c, y.ptr, bra->bond_elems(site) * sizeof(imps::dcplx));
+    }
+    return IMPS_OK;
+  });
+}
+
+int imps_mult_galerkin(imps_mult_envs* E, double* eps) {
+  if (!E || !eps) return IMPS_INVALID_ARG;
+  return guard(E->ctx, [&] {
+    *eps = imps::mult_galerkin(E->ctx, E);
+    return IMPS_OK;
+  });
+}
+
+int imps_mult_sweep(imps_mult_envs* E, double gauge_tol, int gauge_maxiter, double env_tol, int env_maxiter,
+                    double* eps) {
+  if (!E || !eps || gauge_maxiter <= 0 || env_maxiter <= 0) return IMPS_INVALID_ARG;
+  return guard(E->ctx, [&] {
+    *eps = imps::mult_sweep(E->ctx, E, gauge_tol, gauge_maxiter, env_tol, env_maxiter);
+    return IMPS_OK;
+  });
 }
 
 }  // extern "C"

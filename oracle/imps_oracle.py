@@ -60,6 +60,7 @@ __all__ = [
     "timeevompo", "timeevompo_site", "mpo_ring",
     "IDMRG2", "ac2_apply", "VOMPS", "MultCache", "push_ternary_left", "push_ternary_right", "mult_ac",
     "mult_c", "env_start_vector", "mixed_fixedpoints", "mult_galerkin", "svdguess_mult_sites", "mult_sweeps",
+    "mult_local_ac", "mult_local_c",
     "mult", "ac2", "idmrg2_split", "idmrg2_sweep", "idmrg2_groundstate",
 ]
 
