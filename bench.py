@@ -54,6 +54,8 @@ def parse():
                         "tdvp: TFIM quench, TDVP in FP64 and split precision from one ground state; "
                         "batch: 64 TFIM instances of uneven D by batched VUMPS, with dE/dh checks")
     p.add_argument("--tdvp-steps", type=int, default=200)
+    p.add_argument("--mpo-steps", type=int, default=20,
+                   help="tdvp mode: steps of the W^II MPO side run (mult with VOMPS at bond D)")
     p.add_argument("--instances", type=int, default=64)
     p.add_argument("--threads", type=int, default=16)
     p.add_argument("--no-seq", action="store_true")
@@ -534,6 +536,30 @@ def run_tdvp(args, world, rank, local):
         runs[prec] = {"steps_per_s": args.tdvp_steps / t_steps, "s_per_step": t_steps / args.tdvp_steps,
                       "energy_drift_max": float(np.max(np.abs(np.array(es) - E0))), "sx": xs, "sz": zs}
         c.close()
+    # side run: the same quench by the W^II time-evolution MPO applied with mult(W, psi, VOMPS(D))
+    side = None
+    if args.mpo_steps > 0:
+        c = imps.Context(local)
+        psi = imps.CanonicalIMPS(c, [2], [D])
+        for f, a in snap.items():
+            psi.set(f, 0, a)
+        W = imps.timeevompo(H1, dt, "WII")
+        xs_m = [imps.expectationvalue(psi, (1, sx)).real]
+        t_m, iters = 0.0, []
+        for k in range(args.mpo_steps):
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            psi, _, minfo = imps.mult(W, psi, imps.VOMPS(D=D, maxiter=50, tol=args.tol))
+            c.synchronize()
+            t_m += time.perf_counter() - t1
+            iters.append(minfo.niter)
+            xs_m.append(imps.expectationvalue(psi, (1, sx)).real)
+        ref = runs["fp64"]["sx"][:args.mpo_steps + 1]
+        side = {"mpo": "timeevompo(H(h=1.5), -0.01i, WII)", "steps": args.mpo_steps,
+                "steps_per_s": args.mpo_steps / t_m, "vomps_iterations": iters,
+                "max_abs_dsx_vs_tdvp_fp64": float(np.max(np.abs(np.array(xs_m) - np.array(ref)))),
+                "sx": [round(v, 12) for v in xs_m]}
+        c.close()
     dsx = float(np.max(np.abs(np.array(runs["split"]["sx"]) - np.array(runs["fp64"]["sx"]))))
     dsz = float(np.max(np.abs(np.array(runs["split"]["sz"]) - np.array(runs["fp64"]["sz"]))))
     every = max(1, args.tdvp_steps // 20)
@@ -547,7 +573,7 @@ def run_tdvp(args, world, rank, local):
             "ground_state": {"iterations": ginfo.niter, "galerkin": ginfo.itererr, "energy_per_site": e_gs,
                              "wall_s": gs_s},
             "fp64": runs["fp64"], "split": runs["split"], "max_abs_dsx": dsx, "max_abs_dsz": dsz,
-            "sample_every_steps": every}
+            "sample_every_steps": every, "mpo_side_run": side}
 
 
 def run_batch(args, world, rank, local):

@@ -154,17 +154,27 @@ __global__ void k_proj_update(int64_t n, int nv, const dcplx* __restrict__ V, in
 }
 
 // Gram-Schmidt projections against a basis of nv <= NV columns, one kernel per pass.
-// The rows are taken in chunks of GS_ROWS; per chunk the block loads V[chunk, 0:nv]
-// once from HBM (coalesced: 32 consecutive rows per warp and column) into shared
-// memory, optionally applies the pending update w <- w - V h (the column partial sums
-// of each row combined through shared memory), then forms the chunk's contribution
-// to h'_j = <V_j, w> for every column from shared memory, GS_THREADS / NV threads per
-// column.  Few registers per thread: 8 resident blocks of 256 threads per SM keep
-// enough loads in flight for the HBM bandwidth.  Partials: part[blockIdx.x + ldp k],
-// k < 2 nv the dots (re, im interleaved), k = 2 nv the norm^2 of w (after the update).
+// The rows are taken in chunks of GS_ROWS.  A GS_STAGES-deep cp.async ring stages each
+// chunk of V[chunk, 0:nv] and w[chunk] from HBM into shared memory (coalesced: 64
+// consecutive rows per column), so several chunks are in flight per block while the
+// current one is used: the pending update w <- w - V h (the column partial sums of a row
+// combined through shared memory), then the chunk's contribution to h'_j = <V_j, w> for
+// every column, GS_THREADS / NV threads per column.  Few registers per thread.
+// Partials: part[blockIdx.x + ldp k], k < 2 nv the dots (re, im), k = 2 nv the norm^2
+// of w (after the update).
 constexpr int GS_THREADS = 256;
 constexpr int GS_ROWS = 64;
 constexpr int GS_QP = GS_THREADS / GS_ROWS;
+constexpr int GS_STAGES = 3;
+
+template <int NV>
+constexpr size_t gs_smem_bytes() {
+  return (size_t)GS_STAGES * (NV + 1) * GS_ROWS * sizeof(dcplx);
+}
+
+__device__ __forceinline__ void gs_cp16(uint32_t dst, const void* src, int bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+}
 
 template <int NV, bool UPDATE>
 __global__ void __launch_bounds__(GS_THREADS) k_gs_pass(int64_t n, int nv, const dcplx* __restrict__ V, int64_t ldv,
@@ -172,7 +182,8 @@ __global__ void __launch_bounds__(GS_THREADS) k_gs_pass(int64_t n, int nv, const
                                                        double* __restrict__ part, int64_t ldp) {
   constexpr int TPC = GS_THREADS / NV;   // threads per column in the dot phase
   constexpr int RPD = GS_ROWS / TPC;     // rows per thread in the dot phase
-  __shared__ dcplx Vs[NV][GS_ROWS];
+  constexpr int STAGE = (NV + 1) * GS_ROWS;
+  extern __shared__ __align__(16) dcplx gs_sm[];   // [stage][NV + 1][GS_ROWS]: columns, then w
   __shared__ dcplx as[GS_ROWS];
   __shared__ dcplx apart[UPDATE ? GS_QP : 1][GS_ROWS];
   __shared__ dcplx cs[NV];
@@ -180,56 +191,87 @@ __global__ void __launch_bounds__(GS_THREADS) k_gs_pass(int64_t n, int nv, const
   const int tid = threadIdx.x, lane = tid & 31;
   if (UPDATE && tid < NV)
     cs[tid] = tid < nv ? make_double2(-hdev[2 * tid], -hdev[2 * tid + 1]) : make_double2(0.0, 0.0);
-  if (UPDATE) __syncthreads();
-  const int r1 = tid % GS_ROWS, q = tid / GS_ROWS;   // load phase: row r1, columns q + GS_QP u
+  const int r1 = tid % GS_ROWS, q = tid / GS_ROWS;   // load / update phase: row r1, columns q + GS_QP u
   const int jd = tid / TPC, sd = tid % TPC;          // dot phase: column jd, rows sd + TPC u
-  double dre = 0.0, dim = 0.0, nrm = 0.0;
-  for (int64_t base = blockIdx.x * (int64_t)GS_ROWS; base < n; base += (int64_t)gridDim.x * GS_ROWS) {
-    const int64_t i = base + r1;
+  const uint32_t sbase = static_cast<uint32_t>(__cvta_generic_to_shared(gs_sm));
+  const int64_t nchunks = (n + GS_ROWS - 1) / GS_ROWS;
+  auto issue = [&](int stage, int64_t chunk) {
+    const int64_t i = chunk * GS_ROWS + r1;
     const bool ok = i < n;
-    double ar = 0.0, ai = 0.0;
 #pragma unroll
     for (int u = 0; u < NV / GS_QP; ++u) {
       const int j = q + GS_QP * u;
-      const dcplx v = (ok && j < nv) ? V[i + ldv * j] : make_double2(0.0, 0.0);
-      Vs[j][r1] = v;
-      if (UPDATE) {
-        const dcplx c = cs[j];
+      const bool live = ok && j < nv;
+      gs_cp16(sbase + 16u * (uint32_t)(stage * STAGE + j * GS_ROWS + r1), live ? (const void*)(V + i + ldv * j) : V,
+              live ? 16 : 0);
+    }
+    if (q == 0) gs_cp16(sbase + 16u * (uint32_t)(stage * STAGE + NV * GS_ROWS + r1), ok ? (const void*)(w + i) : w,
+                        ok ? 16 : 0);
+  };
+  // chunk t of this block is blockIdx.x + t gridDim.x
+  int64_t t_issue = 0;
+#pragma unroll
+  for (int st = 0; st < GS_STAGES - 1; ++st) {
+    const int64_t c = blockIdx.x + t_issue * gridDim.x;
+    if (c < nchunks) issue(st, c);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    ++t_issue;
+  }
+  double dre = 0.0, dim = 0.0, nrm = 0.0;
+  for (int64_t t = 0;; ++t) {
+    const int64_t chunk = blockIdx.x + t * gridDim.x;
+    if (chunk >= nchunks) break;
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(GS_STAGES - 2) : "memory");
+    __syncthreads();
+    {
+      const int64_t c = blockIdx.x + t_issue * gridDim.x;
+      if (c < nchunks) issue((int)(t_issue % GS_STAGES), c);
+      asm volatile("cp.async.commit_group;\n" ::: "memory");
+      ++t_issue;
+    }
+    const dcplx* Vs = gs_sm + (t % GS_STAGES) * STAGE;
+    const dcplx* ws = Vs + NV * GS_ROWS;
+    const int64_t i = chunk * GS_ROWS + r1;
+    const dcplx* arow = ws;
+    if (UPDATE) {
+      double ar = 0.0, ai = 0.0;
+#pragma unroll
+      for (int u = 0; u < NV / GS_QP; ++u) {
+        const int j = q + GS_QP * u;
+        const dcplx c = cs[j], v = Vs[j * GS_ROWS + r1];
         ar = fma(c.x, v.x, fma(-c.y, v.y, ar));
         ai = fma(c.x, v.y, fma(c.y, v.x, ai));
       }
-    }
-    if (UPDATE) {
       apart[q][r1] = make_double2(ar, ai);
       __syncthreads();
       if (tid < GS_ROWS) {
-        dcplx wi = ok ? w[i] : make_double2(0.0, 0.0);
+        dcplx wi = ws[tid];
 #pragma unroll
-        for (int t = 0; t < GS_QP; ++t) {
-          wi.x += apart[t][tid].x;
-          wi.y += apart[t][tid].y;
+        for (int k = 0; k < GS_QP; ++k) {
+          wi.x += apart[k][tid].x;
+          wi.y += apart[k][tid].y;
         }
-        if (ok) w[i] = wi;
+        if (i < n) w[i] = wi;
         as[tid] = wi;
         nrm = fma(wi.x, wi.x, fma(wi.y, wi.y, nrm));
       }
+      __syncthreads();
+      arow = as;
     } else if (tid < GS_ROWS) {
-      const dcplx wi = ok ? w[i] : make_double2(0.0, 0.0);
-      as[tid] = wi;
+      const dcplx wi = ws[tid];
       nrm = fma(wi.x, wi.x, fma(wi.y, wi.y, nrm));
     }
-    __syncthreads();
     if (jd < nv) {
 #pragma unroll
       for (int u = 0; u < RPD; ++u) {
         const int r = sd + TPC * u;
-        const dcplx v = Vs[jd][r], a = as[r];
+        const dcplx v = Vs[jd * GS_ROWS + r], a = arow[r];
         dre = fma(v.x, a.x, fma(v.y, a.y, dre));
         dim = fma(v.x, a.y, fma(-v.y, a.x, dim));
       }
     }
-    __syncthreads();
   }
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 #pragma unroll
   for (int o = TPC / 2; o >= 1; o >>= 1) {
     dre += __shfl_xor_sync(0xffffffffu, dre, o);
@@ -243,9 +285,9 @@ __global__ void __launch_bounds__(GS_THREADS) k_gs_pass(int64_t n, int nv, const
   if (lane == 0) nred[tid >> 5] = nrm;
   __syncthreads();
   if (tid == 0) {
-    double t = 0.0;
-    for (int k = 0; k < GS_THREADS / 32; ++k) t += nred[k];
-    part[blockIdx.x + ldp * (2 * nv)] = t;
+    double tsum = 0.0;
+    for (int k = 0; k < GS_THREADS / 32; ++k) tsum += nred[k];
+    part[blockIdx.x + ldp * (2 * nv)] = tsum;
   }
 }
 
@@ -597,24 +639,42 @@ double proj_pass(Context* ctx, int64_t n, int nv, const dcplx* V, int64_t ldv, d
 
 namespace {
 template <int NV>
-void launch_gs(Context* ctx, bool update, int nb, int64_t n, int nv, const dcplx* V, int64_t ldv, const double* hdev,
-               dcplx* w, double* part) {
-  if (update)
-    k_gs_pass<NV, true><<<nb, GS_THREADS, 0, ctx->stream>>>(n, nv, V, ldv, hdev, w, part, nb);
-  else
-    k_gs_pass<NV, false><<<nb, GS_THREADS, 0, ctx->stream>>>(n, nv, V, ldv, hdev, w, part, nb);
+int gs_blocks_for(int64_t n) {
+  // resident blocks per SM by shared memory (the ring plus the static arrays), at most 8
+  const int per_sm = std::max(1, std::min(8, (int)((220 * 1024) / (gs_smem_bytes<NV>() + 8 * 1024))));
+  return (int)std::max<int64_t>(1, std::min<int64_t>((n + GS_ROWS - 1) / GS_ROWS, (int64_t)148 * per_sm));
+}
+template <int NV, bool UPDATE>
+void launch_gs_kernel(Context* ctx, int nb, int64_t n, int nv, const dcplx* V, int64_t ldv, const double* hdev,
+                      dcplx* w, double* part, int64_t ldp) {
+  static bool attr = false;  // one device type per process
+  if (!attr) {
+    IMPS_CUDA(cudaFuncSetAttribute(k_gs_pass<NV, UPDATE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)gs_smem_bytes<NV>()));
+    attr = true;
+  }
+  k_gs_pass<NV, UPDATE><<<nb, GS_THREADS, gs_smem_bytes<NV>(), ctx->stream>>>(n, nv, V, ldv, hdev, w, part, ldp);
+}
+int gs_pass_blocks(int64_t n, int nv) {
+  return nv <= 8 ? gs_blocks_for<8>(n) : nv <= 16 ? gs_blocks_for<16>(n) : gs_blocks_for<32>(n);
+}
+void gs_pass(Context* ctx, bool update, int64_t n, int nv, const dcplx* V, int64_t ldv, const double* hdev, dcplx* w,
+             double* part, int64_t ldp, double* out) {
+  const int nb = gs_pass_blocks(n, nv);
+  if (nv <= 8) {
+    if (update) launch_gs_kernel<8, true>(ctx, nb, n, nv, V, ldv, hdev, w, part, ldp);
+    else launch_gs_kernel<8, false>(ctx, nb, n, nv, V, ldv, hdev, w, part, ldp);
+  } else if (nv <= 16) {
+    if (update) launch_gs_kernel<16, true>(ctx, nb, n, nv, V, ldv, hdev, w, part, ldp);
+    else launch_gs_kernel<16, false>(ctx, nb, n, nv, V, ldv, hdev, w, part, ldp);
+  } else {
+    if (update) launch_gs_kernel<32, true>(ctx, nb, n, nv, V, ldv, hdev, w, part, ldp);
+    else launch_gs_kernel<32, false>(ctx, nb, n, nv, V, ldv, hdev, w, part, ldp);
+  }
+  check_launch(ctx);
+  k_final_sum_cols<<<2 * nv + 1, kRedThreads, 0, ctx->stream>>>(nb, part, ldp, out);
   check_launch(ctx);
 }
-void gs_pass(Context* ctx, bool update, int nb, int64_t n, int nv, const dcplx* V, int64_t ldv, const double* hdev,
-             dcplx* w, double* part, double* out) {
-  if (nv <= 8) launch_gs<8>(ctx, update, nb, n, nv, V, ldv, hdev, w, part);
-  else if (nv <= 16) launch_gs<16>(ctx, update, nb, n, nv, V, ldv, hdev, w, part);
-  else launch_gs<32>(ctx, update, nb, n, nv, V, ldv, hdev, w, part);
-  k_final_sum_cols<<<2 * nv + 1, kRedThreads, 0, ctx->stream>>>(nb, part, nb, out);
-  check_launch(ctx);
-}
-// blocks of a Gram-Schmidt pass: one chunk per block at most, 8 blocks per SM
-int gs_blocks(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + GS_ROWS - 1) / GS_ROWS, 148 * 8)); }
 const char* kNonFinite =
     "non-finite value (NaN or Inf) in the Krylov iteration: the operator or the start vector holds one";
 }  // namespace
@@ -640,15 +700,15 @@ double gs_project(Context* ctx, int64_t n, int nv, const dcplx* V, int64_t ldv, 
     }
     return std::sqrt(std::max(nw1, 0.0));
   }
-  const int nb = gs_blocks(n);
+  const int nb = gs_pass_blocks(n, nv);
   const int ncol = 2 * nv + 1;
   DevBuf& part = ctx->buf("gs_part", (size_t)nb * ncol * sizeof(double));
   DevBuf& outb = ctx->buf("gs_out", (size_t)3 * ncol * sizeof(double));
   double* out[3] = {outb.d(), outb.d() + ncol, outb.d() + 2 * ncol};
   ScopedTimer t(ctx, "orth", (double)n * 16 * (nv + 1));
   // projection 1 (dots of w), then its update fused with the dots of projection 2
-  gs_pass(ctx, false, nb, n, nv, V, ldv, nullptr, w, part.d(), out[0]);
-  gs_pass(ctx, true, nb, n, nv, V, ldv, out[0], w, part.d(), out[1]);
+  gs_pass(ctx, false, n, nv, V, ldv, nullptr, w, part.d(), nb, out[0]);
+  gs_pass(ctx, true, n, nv, V, ldv, out[0], w, part.d(), nb, out[1]);
   std::vector<double> hv(2 * ncol);
   download(ctx, hv.data(), out[0], hv.size() * sizeof(double));
   double nw0 = hv[2 * nv], nw1 = hv[ncol + 2 * nv];
@@ -661,7 +721,7 @@ double gs_project(Context* ctx, int64_t n, int nv, const dcplx* V, int64_t ldv, 
   std::vector<double> hn(hv.begin() + ncol, hv.end());
   for (int pass = 1; pass < 3 && nw1 < 0.5 * nw0; ++pass) {
     const int nxt = cur == 1 ? 2 : 1;
-    gs_pass(ctx, true, nb, n, nv, V, ldv, out[cur], w, part.d(), out[nxt]);
+    gs_pass(ctx, true, n, nv, V, ldv, out[cur], w, part.d(), nb, out[nxt]);
     for (int j = 0; j < nv; ++j) h[j] += cplx(hn[2 * j], hn[2 * j + 1]);
     download(ctx, hn.data(), out[nxt], ncol * sizeof(double));
     nw0 = nw1;
