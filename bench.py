@@ -48,7 +48,7 @@ def parse():
                         "residual (the mixed-precision form); fp64: the plain FP64 pipeline")
     p.add_argument("--nslices", type=int, default=0, help="int8 slices (0 = adaptive to the solver tolerance)")
     p.add_argument("--D", type=int, default=WORKLOAD["D"])
-    p.add_argument("--mode", default="vumps", choices=["vumps", "heff", "converge", "tdvp", "batch"],
+    p.add_argument("--mode", default="vumps", choices=["vumps", "heff", "converge", "tdvp", "batch", "kernels"],
                    help="vumps: one VUMPS iteration per step; heff: one AC Heff apply per step; "
                         "converge: VUMPS to convergence in FP64 and split precision from the same start; "
                         "tdvp: TFIM quench, TDVP in FP64 and split precision from one ground state; "
@@ -442,6 +442,59 @@ def run_heff(args, world, rank, local):
             "config": {"workload": "ac_heff_hubbard_jw", "D": D, "precision": args.precision,
                        "nslices": args.nslices if args.precision == "split" else None},
             "kernel_ms": {k: round(v[1] / args.steps, 3) for k, v in prof.items()}}
+
+
+def run_kernels(args, world, rank, local):
+    """The FP64 building blocks around the GEMM engines at the workload's sizes (d = 4):
+    QRpos of the (4 D) x D site matrix of the gauge fix and one restart cycle of the AC
+    Lanczos eigensolve of the Hubbard model (its Gram-Schmidt passes).  Kernel-class times
+    from CUDA events on the context stream (the library's profiler), after one untimed
+    repetition of each."""
+    import torch
+    import infinitempsalgorithms_b200 as imps
+    torch.cuda.set_device(local)
+    ctx = imps.Context(local)
+    D = args.D
+    rng = np.random.default_rng(7)
+    M = np.asfortranarray(rng.standard_normal((4 * D, D)) + 1j * rng.standard_normal((4 * D, D)))
+    imps.qrpos(M, ctx=ctx)
+    ctx.synchronize()
+    ctx.profile(True)
+    ctx.profile_reset()
+    reps = max(1, args.steps)
+    for _ in range(reps):
+        Q, R = imps.qrpos(M, ctx=ctx)
+    ctx.synchronize()
+    qr = ctx.profile_get("qr")
+    zg = ctx.profile_get("zgemm_fp64")
+    ctx.profile(False)
+    qerr = float(np.linalg.norm(Q @ R - M) / np.linalg.norm(M))
+    H = imps.hubbard_hamiltonian()
+    psi = imps.CanonicalIMPS(ctx, [4], [D])
+    envs = imps.DMRGCache(psi, H, build=False)
+    GL = rng.standard_normal((D, 6, D)) + 1j * rng.standard_normal((D, 6, D))
+    GR = rng.standard_normal((D, 6, D)) + 1j * rng.standard_normal((D, 6, D))
+    envs.set_leftenv(1, GL + GL.conj().transpose(2, 1, 0))
+    envs.set_rightenv(1, GR + GR.conj().transpose(2, 1, 0))
+    x0 = np.asfortranarray(rng.standard_normal((D, 4, D)) + 1j * rng.standard_normal((D, 4, D)))
+    hac = imps.AC_hamiltonian(1, psi, H, psi, envs)
+    alg = dict(tol=1e-9, krylovdim=30, maxiter=1, eager=False)
+    imps.fixedpoint(hac, x0, "SR", alg)
+    ctx.synchronize()
+    ctx.profile(True)
+    ctx.profile_reset()
+    imps.fixedpoint(hac, x0, "SR", alg)
+    ctx.synchronize()
+    orth = ctx.profile_get("orth")
+    ctx.profile(False)
+    n = D * 4 * D
+    return {"metric": f"QRpos and Gram-Schmidt kernel times (d=4, D={D})", "unit": "ms",
+            "config": {"workload": "fp64_blocks", "D": D, "qr_shape": [4 * D, D], "krylovdim": 30},
+            "qrpos_ms": qr[1] / reps, "qrpos_tflops": qr[2] / reps / (qr[1] / reps / 1e3) / 1e12 if qr[1] else None,
+            "qrpos_inner_gemm_ms": zg[1] / reps, "qrpos_rel_residual": qerr,
+            "gram_schmidt": {"projections": orth[0], "ms": orth[1],
+                             "min_bytes": orth[2], "vector_bytes": 16 * n,
+                             "gbs_min_bytes": orth[2] / (orth[1] / 1e3) / 1e9 if orth[1] else None}}
 
 
 def run_converge(args, world, rank, local):
@@ -838,6 +891,11 @@ def main():
         return
     if args.mode == "tdvp":
         res = run_tdvp(args, world, rank, local)
+        if rank == 0:
+            print(json.dumps(res))
+        return
+    if args.mode == "kernels":
+        res = run_kernels(args, world, rank, local)
         if rank == 0:
             print(json.dumps(res))
         return
