@@ -1,8 +1,10 @@
 """W^I / W^II time-evolution MPOs (timeevompo, src/algorithms/timeevo/w1w2.jl:26-45).
 
 The reference's per-site kernel lives in an unvendored package, so the oracle
-restates the published construction (arXiv:1407.1832) and parity is unpinned: the
-oracle is checked by the physics, the periodic-trace ring operator of the MPO matching
+restates the published construction (arXiv:1407.1832); tensor-level parity is
+unpinned, and the reference's own tests pin it only through energy conservation under
+the exact application (test/operators/w1w2.jl:1-33, test/algorithms/tdvp.jl:36-43, at
+their tolerances 1e-10 / 1e-4 / 1e-6).  The oracle is further checked by the physics, the periodic-trace ring operator of the MPO matching
 exp(delta H) of the ring up to O(delta^2) (error ratio 4 when delta halves) and the
 identity Hamiltonian giving the identity MPO (test/operators/w1w2.jl:11-17), and the
 library's host routine behind imps_timeevompo_tensor is checked against the oracle
@@ -64,3 +66,41 @@ def test_library_tensor_matches_oracle(alg):
             got = imps.timeevompo(H, delta, alg).Ws[0]
             ref = O.timeevompo(oH, delta, alg)[0]
             assert np.max(np.abs(got - ref)) < 1e-13
+
+
+def _apply_exact(Ws, psi):
+    """``CanonicalIMPS((W * DenseIMPS(psi.AL)).As)`` (test/operators/w1w2.jl:11): the
+    uncompressed product, site tensors ``B[(wl, bl), u, (wr, br)] = sum_d W[wl,u,wr,d]
+    AL[bl,d,br]`` (``operators/linalg.jl:15-20``), then canonical form."""
+    As = []
+    for l, A in enumerate(psi.AL):
+        W = Ws[l % len(Ws)]
+        wl, u, wr, _ = W.shape
+        bl, _, br = A.shape
+        B5 = np.einsum("wurd,bdc->wburc", W, A)
+        As.append(np.asfortranarray(B5.reshape((wl * bl, u, wr * br), order="F")))
+    return O.canonical_from_sites(As)
+
+
+def test_reference_energy_conservation_random_state():
+    # test/operators/w1w2.jl:1-33: a random D=8 two-site state, dt = 0.01; the identity
+    # Hamiltonian's W^I leaves the energy unchanged (1e-10), W^II and W^I keep it within 1e-4
+    H = O.SchurMPO([O.heisenberg_hamiltonian().Ws[0]] * 2)
+    psi0 = O.randomimps([2, 2], D=8, seed=61)
+    e0 = O.expectationvalue(psi0, H, O.build_envs(psi0, H)).real / 2
+    empty = O.SchurMPO([O.mpohamiltonian(np.zeros((2, 2), complex), [])] * 2)
+    out = _apply_exact(O.timeevompo(empty, -0.01j, "WI"), psi0)
+    assert abs(O.expectationvalue(out, H, O.build_envs(out, H)).real / 2 - e0) < 1e-10
+    for alg in ("WII", "WI"):
+        out = _apply_exact(O.timeevompo(H, -0.01j, alg), psi0)
+        assert abs(O.expectationvalue(out, H, O.build_envs(out, H)).real / 2 - e0) < 1e-4
+
+
+def test_reference_energy_conservation_ground_state():
+    # test/algorithms/tdvp.jl:36-43: from the VUMPS ground state, W^II at dt = 0.01 keeps
+    # the energy within 1e-6
+    H = O.SchurMPO([O.heisenberg_hamiltonian().Ws[0]] * 2)
+    psi, envs, _ = O.find_groundstate(O.randomimps([2, 2], D=8, seed=62), H, O.VUMPS(D=8, maxiter=200, tol=1e-10))
+    e0 = O.expectationvalue(psi, H, envs).real / 2
+    out = _apply_exact(O.timeevompo(H, -0.01j, "WII"), psi)
+    assert abs(O.expectationvalue(out, H, O.build_envs(out, H)).real / 2 - e0) < 1e-6
