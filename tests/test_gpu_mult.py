@@ -78,3 +78,21 @@ def test_mult_identity_two_site_cell(ctx):
 def _download(psi):
     N = len(psi)
     return O.CanonicalIMPS(list(psi.AL), list(psi.AR), list(psi.C), list(psi.AC))
+
+
+def test_mult_lossless_bond_equals_naive_product(ctx):
+    # test/algorithms/arithmetics.jl:290-297 on the device: at the lossless bond dimension
+    # mult returns the naive product W . psi
+    H = O.SchurMPO([O.heisenberg_hamiltonian().Ws[0]] * 2)
+    W = O.timeevompo(H, -0.05j, "WII")
+    opsi = O.randomimps([2, 2], D=3, seed=9)
+    As = []
+    for l in range(2):
+        wl, u, wr, _ = W[l].shape
+        bl, _, br = opsi.AL[l].shape
+        B5 = np.einsum("wurd,bdc->wburc", W[l], opsi.AL[l])
+        As.append(np.asfortranarray(B5.reshape((wl * bl, u, wr * br), order="F")))
+    ref = O.canonical_from_sites(As)
+    y, _, info = imps.mult(imps.DenseIMPO(W), upload_state(ctx, opsi), imps.VOMPS(D=12, maxiter=300, tol=1e-10))
+    assert max(y.chi) == 12
+    assert abs(O.state_dot(_download(y), ref)) > 1 - 1e-8

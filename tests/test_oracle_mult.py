@@ -48,3 +48,30 @@ def test_two_site_cell_and_ternary_push_identities():
     A = psi.AL[0]
     np.testing.assert_allclose(O.push_ternary_left(L, A, W[0], A), O.push_mpo_left(L, W[0], A), atol=1e-12)
     np.testing.assert_allclose(O.push_ternary_right(L, A, W[0], A), O.push_mpo_right(L, W[0], A), atol=1e-12)
+
+
+def test_reference_identity_mpo_on_random_state():
+    # test/algorithms/api.jl:502-508: the identity MPO applied to a random N=1 D=6 state at
+    # D = 6 returns it (|<y|psi>| = 1 within 1e-6)
+    psi0 = O.randomimps([2], D=6, seed=42)
+    I = [np.asfortranarray(np.eye(2, dtype=complex).reshape(1, 2, 1, 2))]
+    y, _, _ = O.mult(I, psi0, O.VOMPS(D=6, maxiter=50, tol=1e-10))
+    assert abs(abs(O.state_dot(y, psi0)) - 1) < 1e-6
+
+
+def test_reference_lossless_bond_equals_naive_product():
+    # test/algorithms/arithmetics.jl:290-297: at the lossless bond dimension the result is
+    # the naive product W . psi (fidelity > 1 - 1e-8)
+    H = O.SchurMPO([O.heisenberg_hamiltonian().Ws[0]] * 2)
+    W = O.timeevompo(H, -0.05j, "WII")
+    psi = O.randomimps([2, 2], D=3, seed=9)
+    As = []
+    for l in range(2):
+        wl, u, wr, _ = W[l].shape
+        bl, _, br = psi.AL[l].shape
+        B5 = np.einsum("wurd,bdc->wburc", W[l], psi.AL[l])
+        As.append(np.asfortranarray(B5.reshape((wl * bl, u, wr * br), order="F")))
+    ref = O.canonical_from_sites(As)
+    y, _, info = O.mult(W, psi, O.VOMPS(D=12, maxiter=300, tol=1e-10))
+    assert max(a.shape[2] for a in y.AL) == 12
+    assert abs(O.state_dot(y, ref)) > 1 - 1e-8
