@@ -67,6 +67,8 @@ def parse():
     p.add_argument("--seed", type=int, default=None)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--cpu-full", action="store_true",
+                   help="cpu_baseline from a whole oracle VUMPS iteration (minutes at D=1024) instead of a sample")
     p.add_argument("--fp64-steps", type=int, default=None,
                    help="iterations of the plain FP64 arm timed beside the split run (default: --steps; 0 = skip)")
     p.add_argument("--ref-steps", type=int, default=1,
@@ -182,10 +184,14 @@ def fp64_reference_tflops():
     return 8.0 * 4096 * 4096 * 1024 / (ms / 1e3) / 1e12
 
 
-# DRAM bytes per k_gemm_i8 launch, from one ncu capture of the AC Heff of this
-# workload (profiles/); None until a capture of the current kernel exists.
-GEMM_I8_TRAFFIC_PER_LAUNCH = None
-GEMM_I8_TRAFFIC_SOURCE = None
+# DRAM bytes per k_gemm_i8 launch: the mean of the two launches of one AC Heff apply at
+# Hubbard D=1024, s=5 (GL x: 319 MB read + 382 MB written; T2 GR: 979 MB read + 59 MB
+# written), from one ncu capture (profiles/k_gemm_i8_ac_heff_hubbard_d1024_traffic.md).
+# The algorithmic bytes of the same two launches are 573 MB and 633 MB.
+GEMM_I8_TRAFFIC_PER_LAUNCH = 0.5 * (318806528 + 381801472 + 978851840 + 58522112)
+GEMM_I8_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum, mean of the 2 k_gemm_i8 launches of "
+                          "one AC Heff apply (Hubbard D=1024, s=5; bench.py --mode heff --D 1024); the timed "
+                          "region mixes these with the smaller C-Heff and push launches")
 
 
 def ac_flops(D, d, w):
@@ -526,6 +532,9 @@ def run_converge(args, world, rank, local):
         dt = time.perf_counter() - t0
         out[prec] = {"iterations": info.niter, "converged": bool(info.converged), "galerkin": info.itererr,
                      "energy_per_site": e, "wall_s": dt, "s_per_iter": dt / max(info.niter, 1)}
+        if rank == 0:
+            # each arm as soon as it ends, so that a run cut short still reports the first
+            print(json.dumps({"arm": prec, **out[prec]}), file=sys.stderr, flush=True)
         ctx.close()
     res = {"metric": f"VUMPS to convergence ({args.model}, N={N}, D={args.D}, tol={args.tol})",
            "config": {"model": args.model, "N": N, "D": args.D, "seed": seed, "tol": args.tol,
@@ -836,6 +845,55 @@ def oracle_iterations(opsi, oH, oenvs, eps, k, D):
     return secs, eps
 
 
+def oracle_sample(opsi, oH, oenvs, counts, D, reps=2):
+    """A bounded sample of the oracle's VUMPS iteration (about half a minute of CPU work):
+    ``reps`` AC and C Heff applies, one Gram-Schmidt projection against a 15-vector basis
+    of the AC size, one QRpos of the (4 D) x D site matrix and one (D x 4 D) x D complex
+    product, each timed on the host clock, scaled by this run's per-iteration operation
+    counts (AC / C applies, one projection per apply, QRs, the remaining GEMM flops)."""
+    import oracle as O
+    N = len(opsi)
+    GL, GR, W = oenvs.lefts[0], oenvs.rights[0], oH[0]
+    t = time.perf_counter()
+    for _ in range(reps):
+        O.ac_apply(GL, W, GR, opsi.AC[0])
+    t_ac = (time.perf_counter() - t) / reps
+    GLc = oenvs.lefts[1 % N]
+    t = time.perf_counter()
+    for _ in range(reps):
+        O.c_apply(GLc, GR, opsi.C[0])
+    t_c = (time.perf_counter() - t) / reps
+    n = opsi.AC[0].size
+    basis = O.imps_oracle._KBasis(n, 16)
+    rng = np.random.default_rng(0)
+    for _ in range(15):
+        v = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+        v, _ = O.imps_oracle._cgs2(basis, v / np.linalg.norm(v))
+        basis.append(v / np.linalg.norm(v))
+    w = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    t = time.perf_counter()
+    O.imps_oracle._cgs2(basis, w)
+    t_gs = time.perf_counter() - t
+    M = np.asfortranarray(opsi.AC[0].reshape((-1, opsi.AC[0].shape[2]), order="F"))
+    t = time.perf_counter()
+    O.qrpos(M)
+    t_qr = time.perf_counter() - t
+    t = time.perf_counter()
+    X = M @ opsi.C[0]
+    t_mm = time.perf_counter() - t
+    gemm_rate = 8.0 * M.shape[0] * M.shape[1] * opsi.C[0].shape[1] / t_mm
+    sec = (counts["ac"] * (t_ac + t_gs) + counts["c"] * (t_c + t_gs) + counts["qr"] * t_qr
+           + counts["other_gemm_flops"] / gemm_rate)
+    del X
+    sample = (f"oracle (NumPy/OpenBLAS, {cpu_threads()} threads) op times at D={D} from the GPU run's start state: "
+              f"AC apply {t_ac:.2f} s, C apply {t_c:.2f} s, Gram-Schmidt projection (15 vectors) {t_gs:.2f} s, "
+              f"QRpos {M.shape[0]}x{M.shape[1]} {t_qr:.2f} s, ZGEMM {gemm_rate / 1e9:.0f} GFLOP/s; scaled by this "
+              f"run's per-iteration counts ({counts['ac']:.0f} AC, {counts['c']:.0f} C, {counts['qr']:.0f} QR, "
+              f"{counts['other_gemm_flops'] / 1e12:.1f} TFLOP other GEMM) to {sec:.0f} s per iteration; "
+              f"`--cpu-full` times a whole oracle iteration instead")
+    return sec, sample
+
+
 def run_reference(args, world, rank):
     """The reference arm: the CPU oracle (NumPy/OpenBLAS restatement of the
     reference's VUMPS; Julia is absent) on the same seeded workload.  Preparation
@@ -911,11 +969,14 @@ def main():
         import oracle as O
         opsi, oenvs = oracle_from_snapshot(snap0, WORKLOAD["N"])
         oH = O.SchurMPO([O.hubbard_hamiltonian().Ws[0]] * WORKLOAD["N"])
-        secs, _ = oracle_iterations(opsi, oH, oenvs, eps0, 1, args.D)
-        res["cpu_baseline"] = {"value": 1.0 / secs[0], "unit": UNIT, "cores": cpu_threads(), "kind": "port",
-                               "sample": (f"VUMPS iteration 1 of the oracle (NumPy/OpenBLAS) at D={args.D} from the "
-                                          f"GPU run's seeded canonical start, timed on the host clock "
-                                          f"({secs[0]:.1f} s)")}
+        if args.cpu_full:
+            secs, _ = oracle_iterations(opsi, oH, oenvs, eps0, 1, args.D)
+            sec, sample = secs[0], (f"VUMPS iteration 1 of the oracle (NumPy/OpenBLAS) at D={args.D} from the "
+                                    f"GPU run's seeded canonical start, timed on the host clock ({secs[0]:.1f} s)")
+        else:
+            sec, sample = oracle_sample(opsi, oH, oenvs, res["op_counts_per_iter"], args.D)
+        res["cpu_baseline"] = {"value": 1.0 / sec, "unit": UNIT, "cores": cpu_threads(), "kind": "port",
+                               "sample": sample}
     if rank == 0:
         print(json.dumps(res))
 
