@@ -133,11 +133,18 @@ __global__ void __launch_bounds__(NT, 2)
 // conjugate of an operand only flips the sign of its imaginary fragment.
 // Shared tiles are k-major rows of double2 with one element of padding.
 // ---------------------------------------------------------------------------
+// Tile shapes of the DMMA engine: TM = 128 (8 warps, one CTA per SM by registers and
+// shared memory) for large grids; TM = 64 (4 warps, two CTAs per SM) for grids that would
+// not fill the SMs twice over with 128-row tiles (the skinny products of the blocked QR).
 namespace dm {
-constexpr int BM = 128, BN = 64, BK = 16, STAGES = 3, NT = 256;
-constexpr int LDA = BM + 1, LDB = BN + 1;
-constexpr int A_ELEMS = BK * LDA, B_ELEMS = BK * LDB;
-constexpr int SMEM = STAGES * (A_ELEMS + B_ELEMS) * 16;
+constexpr int BN = 64, BK = 16, STAGES = 3;
+template <int TM>
+struct Tile {
+  static constexpr int BM = TM, NT = 2 * TM, WM = TM / 32;
+  static constexpr int LDA = BM + 1, LDB = BN + 1;
+  static constexpr int A_ELEMS = BK * LDA, B_ELEMS = BK * LDB;
+  static constexpr int SMEM = STAGES * (A_ELEMS + B_ELEMS) * 16;
+};
 }  // namespace dm
 
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, int bytes) {
@@ -153,46 +160,47 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
                : "d"(a), "d"(b));
 }
 
-template <int OPA, int OPB, bool BETA>
-__global__ void __launch_bounds__(dm::NT, 1)
+template <int OPA, int OPB, bool BETA, int TM>
+__global__ void __launch_bounds__(2 * TM, 128 / TM)
     k_zgemm_dmma(int M, int N, int K, double2 alpha, const double2* __restrict__ A, int64_t lda, int64_t sA,
                  const double2* __restrict__ B, int64_t ldb, int64_t sB, double2 beta, double2* __restrict__ C,
                  int64_t ldc, int64_t sC) {
+  using T = dm::Tile<TM>;
   extern __shared__ __align__(16) double2 smem_dm[];
-  double2* As = smem_dm;                              // [STAGES][BK][LDA]
-  double2* Bs = smem_dm + dm::STAGES * dm::A_ELEMS;   // [STAGES][BK][LDB]
+  double2* As = smem_dm;                             // [STAGES][BK][LDA]
+  double2* Bs = smem_dm + dm::STAGES * T::A_ELEMS;   // [STAGES][BK][LDB]
   const int bz = blockIdx.z;
   A += sA * bz;
   B += sB * bz;
   C += sC * bz;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int wm = warp & 3, wn = warp >> 2;  // warp tile origin (32 * wm, 32 * wn)
-  const int m0 = blockIdx.x * dm::BM, n0 = blockIdx.y * dm::BN;
+  const int wm = warp % T::WM, wn = warp / T::WM;  // warp tile origin (32 * wm, 32 * wn)
+  const int m0 = blockIdx.x * T::BM, n0 = blockIdx.y * dm::BN;
   const uint32_t sbase = static_cast<uint32_t>(__cvta_generic_to_shared(smem_dm));
 
   auto issue = [&](int stage, int k0) {
-    // A tile: BM x BK complex, 8 per thread
-    static_assert(dm::BM == 128 && dm::BN == 64 && dm::BK == 16 && dm::NT == 256, "load mapping assumes this tile");
+    // A tile: BM x BK complex, 8 per thread (NT = 2 BM)
+    static_assert(dm::BN == 64 && dm::BK == 16 && (TM == 64 || TM == 128), "load mapping assumes these tiles");
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
       int m, k;
-      if (OPA == OP_N) { m = tid & 127; k = (tid >> 7) + 2 * r; }
-      else { k = tid & 15; m = (tid >> 4) + 16 * r; }
+      if (OPA == OP_N) { m = tid & (TM - 1); k = (tid / TM) + 2 * r; }
+      else { k = tid & 15; m = (tid >> 4) + (T::NT / 16) * r; }
       const int gm = m0 + m, gk = k0 + k;
       const bool ok = gm < M && gk < K;
       const double2* src = ok ? ((OPA == OP_N) ? A + gm + lda * (int64_t)gk : A + gk + lda * (int64_t)gm) : A;
-      cp_async16(sbase + 16u * (stage * dm::A_ELEMS + k * dm::LDA + m), src, ok ? 16 : 0);
+      cp_async16(sbase + 16u * (stage * T::A_ELEMS + k * T::LDA + m), src, ok ? 16 : 0);
     }
-    // B tile: BK x BN complex, 4 per thread
+    // B tile: BK x BN complex, 1024 / NT per thread
 #pragma unroll
-    for (int r = 0; r < 4; ++r) {
+    for (int r = 0; r < 1024 / T::NT; ++r) {
       int n, k;
-      if (OPB == OP_N) { k = tid & 15; n = (tid >> 4) + 16 * r; }
-      else { n = tid & 63; k = (tid >> 6) + 4 * r; }
+      if (OPB == OP_N) { k = tid & 15; n = (tid >> 4) + (T::NT / 16) * r; }
+      else { n = tid & 63; k = (tid >> 6) + (T::NT / 64) * r; }
       const int gn = n0 + n, gk = k0 + k;
       const bool ok = gn < N && gk < K;
       const double2* src = ok ? ((OPB == OP_N) ? B + gk + ldb * (int64_t)gn : B + gn + ldb * (int64_t)gk) : B;
-      cp_async16(sbase + 16u * (dm::STAGES * dm::A_ELEMS + stage * dm::B_ELEMS + k * dm::LDB + n), src, ok ? 16 : 0);
+      cp_async16(sbase + 16u * (dm::STAGES * T::A_ELEMS + stage * T::B_ELEMS + k * T::LDB + n), src, ok ? 16 : 0);
     }
   };
 
@@ -217,21 +225,21 @@ __global__ void __launch_bounds__(dm::NT, 1)
       if (nk < ktiles) issue(nk % dm::STAGES, nk * dm::BK);
       cp_async_commit();
     }
-    const double2* as = As + (kt % dm::STAGES) * dm::A_ELEMS;
-    const double2* bs = Bs + (kt % dm::STAGES) * dm::B_ELEMS;
+    const double2* as = As + (kt % dm::STAGES) * T::A_ELEMS;
+    const double2* bs = Bs + (kt % dm::STAGES) * T::B_ELEMS;
 #pragma unroll
     for (int kb = 0; kb < dm::BK; kb += 4) {
       double ar[4], ai[4], nai[4], br[4], bi[4];
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
-        const double2 v = as[(kb + fk) * dm::LDA + 32 * wm + 8 * i + fr];
+        const double2 v = as[(kb + fk) * T::LDA + 32 * wm + 8 * i + fr];
         ar[i] = v.x;
         ai[i] = (OPA == OP_C) ? -v.y : v.y;
         nai[i] = -ai[i];
       }
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        const double2 v = bs[(kb + fk) * dm::LDB + 32 * wn + 8 * j + fr];
+        const double2 v = bs[(kb + fk) * T::LDB + 32 * wn + 8 * j + fr];
         br[j] = v.x;
         bi[j] = (OPB == OP_C) ? -v.y : v.y;
       }
@@ -277,6 +285,26 @@ __global__ void __launch_bounds__(dm::NT, 1)
   }
 }
 
+template <int OPA, int OPB, int TM>
+void launch_dmma(Context* ctx, int M, int N, int K, double2 alpha, const dcplx* A, int64_t lda, int64_t sA,
+                 const dcplx* B, int64_t ldb, int64_t sB, double2 beta, dcplx* C, int64_t ldc, int64_t sC, int batch,
+                 bool use_beta) {
+  using T = dm::Tile<TM>;
+  // the dynamic shared-memory opt-in is per device and per kernel instance; setting it
+  // twice (two host threads racing here) is harmless
+  static std::atomic<uint64_t> attr_set[2];
+  auto kern = use_beta ? k_zgemm_dmma<OPA, OPB, true, TM> : k_zgemm_dmma<OPA, OPB, false, TM>;
+  const uint64_t bit = 1ull << (ctx->device & 63);
+  std::atomic<uint64_t>& done = attr_set[use_beta ? 1 : 0];
+  if (!(done.load() & bit)) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, T::SMEM);
+    if (e != cudaSuccess) throw Error(IMPS_CUDA_ERROR, std::string("zgemm smem opt-in: ") + cudaGetErrorString(e));
+    done.fetch_or(bit);
+  }
+  dim3 grid((M + T::BM - 1) / T::BM, (N + dm::BN - 1) / dm::BN, batch);
+  kern<<<grid, T::NT, T::SMEM, ctx->stream>>>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC);
+}
+
 template <int OPA, int OPB>
 void launch(Context* ctx, int M, int N, int K, double2 alpha, const dcplx* A, int64_t lda, int64_t sA,
             const dcplx* B, int64_t ldb, int64_t sB, double2 beta, dcplx* C, int64_t ldc, int64_t sC, int batch,
@@ -290,19 +318,12 @@ void launch(Context* ctx, int M, int N, int K, double2 alpha, const dcplx* A, in
                                                               sC);
     return;
   }
-  // the dynamic shared-memory opt-in is per device and per kernel instance; setting it
-  // twice (two host threads racing here) is harmless
-  static std::atomic<uint64_t> attr_set[2];
-  auto kern = use_beta ? k_zgemm_dmma<OPA, OPB, true> : k_zgemm_dmma<OPA, OPB, false>;
-  const uint64_t bit = 1ull << (ctx->device & 63);
-  std::atomic<uint64_t>& done = attr_set[use_beta ? 1 : 0];
-  if (!(done.load() & bit)) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, dm::SMEM);
-    if (e != cudaSuccess) throw Error(IMPS_CUDA_ERROR, std::string("zgemm smem opt-in: ") + cudaGetErrorString(e));
-    done.fetch_or(bit);
-  }
-  dim3 grid((M + dm::BM - 1) / dm::BM, (N + dm::BN - 1) / dm::BN, batch);
-  kern<<<grid, dm::NT, dm::SMEM, ctx->stream>>>(M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC);
+  // 128-row tiles unless they would give fewer than two CTAs per SM; then 64-row tiles,
+  // two of which fit an SM
+  const int64_t tiles128 = (int64_t)((M + 127) / 128) * ((N + dm::BN - 1) / dm::BN) * batch;
+  if (tiles128 >= 2 * 148) launch_dmma<OPA, OPB, 128>(ctx, M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC,
+                                                       batch, use_beta);
+  else launch_dmma<OPA, OPB, 64>(ctx, M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, batch, use_beta);
 }
 
 }  // namespace
