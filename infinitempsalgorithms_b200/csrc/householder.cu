@@ -353,12 +353,11 @@ template <int NB, int RPT>
 void launch_panel(Context* ctx, int R, int b, int zabove, dcplx* A, int64_t lda, dcplx* V, int64_t ldv, dcplx* tau,
                   dcplx* T, int ldt) {
   static_assert(NB * RPT == QR_NBMAX, "panel shared-memory size");
-  static bool attr = false;  // set once per process (one device type)
-  if (!attr) {
+  static DeviceOnce attr;
+  attr.run(ctx->device, [] {
     IMPS_CUDA(cudaFuncSetAttribute(k_qr_panel<NB, RPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)QR_PANEL_SMEM));
-    attr = true;
-  }
+  });
   k_qr_panel<NB, RPT><<<QR_CL, QR_NT, QR_PANEL_SMEM, ctx->stream>>>(R, b, zabove, A, lda, V, ldv, tau, T, ldt);
   ctx->n_kernels++;
   cudaError_t e = cudaPeekAtLastError();

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <complex>
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <map>
@@ -189,6 +190,19 @@ struct Fp64Scope {
   explicit Fp64Scope(Context* c) : ctx(c) { ctx->force_fp64++; }
   ~Fp64Scope() { ctx->force_fp64--; }
 };
+// One-time per-device setup (kernel attributes) safe to reach from several host threads:
+// the setup may run more than once when threads race, so it must be idempotent.
+struct DeviceOnce {
+  std::atomic<uint64_t> done{0};
+  template <class F>
+  void run(int device, F&& f) {
+    const uint64_t bit = 1ull << (device & 63);
+    if (done.load(std::memory_order_acquire) & bit) return;
+    f();
+    done.fetch_or(bit, std::memory_order_release);
+  }
+};
+
 // Inside an Fp64Scope: lets the split engine serve the GEMMs at accuracy tol while alive,
 // when the context runs the split engine with adaptive slice counts (the slice count then
 // follows tol; a fixed count could not reach an arbitrary tolerance).

@@ -647,12 +647,11 @@ int gs_blocks_for(int64_t n) {
 template <int NV, bool UPDATE>
 void launch_gs_kernel(Context* ctx, int nb, int64_t n, int nv, const dcplx* V, int64_t ldv, const double* hdev,
                       dcplx* w, double* part, int64_t ldp) {
-  static bool attr = false;  // one device type per process
-  if (!attr) {
+  static DeviceOnce attr;
+  attr.run(ctx->device, [] {
     IMPS_CUDA(cudaFuncSetAttribute(k_gs_pass<NV, UPDATE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)gs_smem_bytes<NV>()));
-    attr = true;
-  }
+  });
   k_gs_pass<NV, UPDATE><<<nb, GS_THREADS, gs_smem_bytes<NV>(), ctx->stream>>>(n, nv, V, ldv, hdev, w, part, ldp);
 }
 int gs_pass_blocks(int64_t n, int nv) {
