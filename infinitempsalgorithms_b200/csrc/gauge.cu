@@ -42,6 +42,29 @@ double diff_norm(Context* ctx, int64_t n, const dcplx* a, const dcplx* b) {
   return dznrm2(ctx, n, T.z());
 }
 
+// The transfer-matrix eigensolve of a gauge sweep.  Its fixed point only seeds the next
+// sweep, whose own FP64 convergence test decides, so the products may run on the split
+// engine at a tenth of the eigensolver tolerance (the site tensors are constant over the
+// eigensolve: their splits are cached).  When that tolerance needs FP64 products, a
+// split-engine solve to 1e-8 seeds the FP64 solve, which then needs fewer FP64 products
+// for the same convergence test.
+void gauge_eigsolve(Context* ctx, int64_t n, const LinOp& op, const dcplx* c0, dcplx* ev, double etol,
+                    const std::vector<const void*>& cptrs) {
+  ConstScope cs(ctx, cptrs);
+  const bool split = ctx->precision == PREC_SPLIT_I8 && ctx->adaptive_slices;
+  if (split && etol < 1e-8 && slices_for_tol(0.1 * etol) >= 7) {
+    DevBuf& seed = ctx->buf("gauge_seed", (size_t)n * sizeof(dcplx));
+    {
+      SplitAllowScope sa(ctx, 1e-9);
+      arnoldi_dominant(ctx, n, op, c0, seed.z(), 1e-8, 30, 300, true);
+    }
+    arnoldi_dominant(ctx, n, op, seed.z(), ev, etol, 30, 300, true);
+    return;
+  }
+  SplitAllowScope sa(ctx, 0.1 * etol);
+  arnoldi_dominant(ctx, n, op, c0, ev, etol, 30, 300, true);
+}
+
 }  // namespace
 
 GaugeResult uniform_leftorth(Context* ctx, imps_state* st, const std::vector<const dcplx*>& A, const dcplx* C0,
@@ -80,17 +103,12 @@ GaugeResult uniform_leftorth(Context* ctx, imps_state* st, const std::vector<con
       };
       DevBuf& ev = ctx->buf("gauge_evec", (size_t)DN * DN * sizeof(dcplx));
       {
-        // the fixed point only seeds the next sweep, whose own FP64 convergence test decides;
-        // its transfer products may run on the split engine at a tenth of the eigensolver
-        // tolerance (the site tensors are constant over the eigensolve: splits cached)
         std::vector<const void*> cptrs;
         for (int l = 0; l < N; ++l) {
           cptrs.push_back(Aw[l]);
           cptrs.push_back(st->AL[l].ptr);
         }
-        ConstScope cs(ctx, cptrs);
-        SplitAllowScope sa(ctx, 0.1 * etol);
-        arnoldi_dominant(ctx, (int64_t)DN * DN, op, st->C[N - 1].z(), ev.z(), etol, 30, 300, true);
+        gauge_eigsolve(ctx, (int64_t)DN * DN, op, st->C[N - 1].z(), ev.z(), etol, cptrs);
       }
       DevBuf& q = ctx->buf("gauge_q", (size_t)DN * DN * sizeof(dcplx));
       qrpos(ctx, DN, DN, ev.z(), DN, q.z(), st->C[N - 1].z());
@@ -151,17 +169,12 @@ GaugeResult uniform_rightorth(Context* ctx, imps_state* st, const std::vector<co
       };
       DevBuf& ev = ctx->buf("gauge_evec", (size_t)DN * DN * sizeof(dcplx));
       {
-        // the fixed point only seeds the next sweep, whose own FP64 convergence test decides;
-        // its transfer products may run on the split engine at a tenth of the eigensolver
-        // tolerance (the site tensors are constant over the eigensolve: splits cached)
         std::vector<const void*> cptrs;
         for (int l = 0; l < N; ++l) {
           cptrs.push_back(Aw[l]);
           cptrs.push_back(st->AR[l].ptr);
         }
-        ConstScope cs(ctx, cptrs);
-        SplitAllowScope sa(ctx, 0.1 * etol);
-        arnoldi_dominant(ctx, (int64_t)DN * DN, op, st->C[N - 1].z(), ev.z(), etol, 30, 300, true);
+        gauge_eigsolve(ctx, (int64_t)DN * DN, op, st->C[N - 1].z(), ev.z(), etol, cptrs);
       }
       DevBuf& q = ctx->buf("gauge_q", (size_t)DN * DN * sizeof(dcplx));
       lqpos(ctx, DN, DN, ev.z(), DN, st->C[N - 1].z(), q.z());

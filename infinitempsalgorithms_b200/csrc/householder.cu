@@ -279,8 +279,15 @@ struct PanelList {
   short w[QR_NBO / 2];
 };
 
+// T, G and the panels' products live in shared memory for the whole merge (one CTA).
+constexpr size_t QR_MERGE_SMEM = (size_t)2 * QR_NBO * (QR_NBO + 1) * sizeof(dcplx);
+
 __global__ void __launch_bounds__(256) k_merge_t(int bo, PanelList pl, const dcplx* __restrict__ Tin,
                                                  const dcplx* __restrict__ G, dcplx* __restrict__ Tb) {
+  extern __shared__ __align__(16) dcplx msm[];
+  const int ld = bo + 1;
+  dcplx* Ts = msm;                            // Ts[r + ld c]
+  dcplx* Gs = msm + (size_t)QR_NBO * (QR_NBO + 1);
   __shared__ dcplx Xs[QR_NBO][QR_NBMAX];
   const int tid = threadIdx.x;
   for (int e = tid; e < bo * bo; e += blockDim.x) {
@@ -290,7 +297,8 @@ __global__ void __launch_bounds__(256) k_merge_t(int bo, PanelList pl, const dcp
     const int o = pl.off[t];
     dcplx v = make_double2(0.0, 0.0);
     if (r >= o && r < o + pl.w[t]) v = Tin[(size_t)t * QR_NBMAX * QR_NBMAX + (r - o) + QR_NBMAX * (c - o)];
-    Tb[r + (int64_t)bo * c] = v;
+    Ts[r + ld * c] = v;
+    if (pl.n > 1) Gs[r + ld * c] = G[r + (int64_t)bo * c];
   }
   __syncthreads();
   for (int t = 1; t < pl.n; ++t) {
@@ -298,27 +306,28 @@ __global__ void __launch_bounds__(256) k_merge_t(int bo, PanelList pl, const dcp
     const dcplx* Tt = Tin + (size_t)t * QR_NBMAX * QR_NBMAX;
     for (int e = tid; e < c0 * bt; e += blockDim.x) {
       const int r = e % c0, u = e / c0;
-      dcplx s = make_double2(0.0, 0.0);
+      dcplx sacc = make_double2(0.0, 0.0);
       for (int l = r; l < c0; ++l) {
-        const dcplx p = cmul(Tb[r + (int64_t)bo * l], G[l + (int64_t)bo * (c0 + u)]);
-        s.x += p.x;
-        s.y += p.y;
+        const dcplx p = cmul(Ts[r + ld * l], Gs[l + ld * (c0 + u)]);
+        sacc.x += p.x;
+        sacc.y += p.y;
       }
-      Xs[r][u] = s;
+      Xs[r][u] = sacc;
     }
     __syncthreads();
     for (int e = tid; e < c0 * bt; e += blockDim.x) {
       const int r = e % c0, u = e / c0;
-      dcplx s = make_double2(0.0, 0.0);
+      dcplx sacc = make_double2(0.0, 0.0);
       for (int v = 0; v <= u; ++v) {
         const dcplx p = cmul(Xs[r][v], Tt[v + QR_NBMAX * u]);
-        s.x += p.x;
-        s.y += p.y;
+        sacc.x += p.x;
+        sacc.y += p.y;
       }
-      Tb[r + (int64_t)bo * (c0 + u)] = make_double2(-s.x, -s.y);
+      Ts[r + ld * (c0 + u)] = make_double2(-sacc.x, -sacc.y);
     }
     __syncthreads();
   }
+  for (int e = tid; e < bo * bo; e += blockDim.x) Tb[e] = Ts[(e % bo) + ld * (e / bo)];
 }
 
 __global__ void k_extract_r(int k, int n, const dcplx* __restrict__ A, int64_t lda, dcplx* __restrict__ R,
@@ -466,7 +475,11 @@ void qrpos(Context* ctx, int m, int n, const dcplx* M, int64_t ldm, dcplx* Q, dc
     dcplx* Vblk = Vb.z() + P + (int64_t)m * P;
     dcplx* Tb = Tbig.z() + (size_t)blocks.size() * QR_NBO * QR_NBO;
     if (pl.n > 1) gemm_xhv(ctx, bo, bo, RrB, Vblk, Vblk, m, Pb.z(), Gb.z());
-    k_merge_t<<<1, 256, 0, ctx->stream>>>(bo, pl, Tin.z(), Gb.z(), Tb);
+    static DeviceOnce merge_attr;
+    merge_attr.run(ctx->device, [] {
+      IMPS_CUDA(cudaFuncSetAttribute(k_merge_t, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)QR_MERGE_SMEM));
+    });
+    k_merge_t<<<1, 256, QR_MERGE_SMEM, ctx->stream>>>(bo, pl, Tin.z(), Gb.z(), Tb);
     ctx->n_kernels++;
     const int n2 = n - (P + bo);
     if (n2 > 0) {

@@ -125,8 +125,8 @@ struct Context {
   std::vector<double> pending_flops;
   // counters
   int64_t n_ac_apply = 0, n_c_apply = 0, n_push = 0, n_gemm = 0, n_kernels = 0, n_qr = 0;
-  double gemm_flops = 0.0;
-  double qr_flops = 0.0;    // real flops of the Householder QRpos factorizations (geqrf + ungqr)  // real flops of every complex GEMM requested (8 M N K), either precision
+  double gemm_flops = 0.0;  // real flops of every complex GEMM requested (8 M N K), either precision
+  double qr_flops = 0.0;    // real flops of the Householder QRpos factorizations (factor + Q)
   int num_sms = 148;
   // split-precision state
   double split_tol = 1e-10;            // accuracy requested by the running solver
@@ -237,6 +237,8 @@ struct TolScope {
 // Slices the split engine would use right now (0 = FP64 engine).  Adaptive mode picks
 // the smallest s whose truncation floor meets ctx->split_tol; s >= 7 falls back to FP64.
 int active_slices(const Context* ctx);
+// the smallest slice count whose truncation floor meets tol (7 or more: the FP64 engine)
+int slices_for_tol(double tol);
 // Relative accuracy of the GEMM engine currently selected (0 for FP64).
 double split_floor(const Context* ctx);
 
