@@ -13,27 +13,24 @@
 // epilogue adds r_i c_j 2^-7(d+2) acc to the FP64 output.  Truncation error per
 // element is below 2^-7s of the row/column scale.
 //
-// GEMM kernel: persistent, one CTA per SM, warp-specialised, 128 x 64 output tiles.
+// GEMM kernel: persistent, one CTA per SM, warp-specialised, 128 x BN output tiles.
 // K runs outermost: one pipeline stage holds a 64-byte K block of *every* slice
 // plane of both operands, and the MMA thread issues all slice pairs (ta, tb) with
 // ta + tb < s for it, each diagonal d = ta + tb into its own int32 TMEM
-// accumulator (s x 64 columns per tile).  Every byte brought into shared memory
+// accumulator (s x BN columns per tile).  Every byte brought into shared memory
 // thus feeds (s + 1) / 2 MMAs on average instead of one, which is what keeps the
 // tensor pipe fed from L2.
+// Tile width: an M=128 MMA reads its A tile (4 KB per K=32) and B tile (BN x 32 B)
+// from shared memory, whose 128 B/clk per SM feed the int8 pipe's ~7.7k MAC/clk only
+// when BN >= ~115.  BN = 128 is used for s <= 4 (s x 128 TMEM columns still fit the
+// 512 of an SM); BN = 64 for more slices, where the MMA waits on shared memory.
 //   warp 0: TMA producer (cp.async.bulk.tensor, 64B swizzle, 2-8 stages by s)
-//   warp 1: TMEM allocator + single-thread tcgen05.mma issuer (M=128, N=64, K=32)
-//   warps 2-9: epilogue, tcgen05.ld 32x32b, two warps per TMEM lane quarter; each
-//           thread keeps the FP64 sums of its row over all diagonals in registers
-//           and writes the tile once.  With s <= 4 two tiles' accumulators fit in
-//           TMEM, so the epilogue of one tile overlaps the MMAs of the next.
-// The K extent is cut into groups so that no int32 sum can overflow: the largest
-// diagonal adds s pairs, so a group spans fewer than 2^31 / (127^2 s) bytes.
-// Every mbarrier wait of the pipeline is bounded (GemmArgs::wait_cycles of clock64,
-// ~1 s by default); on expiry the kernel sets the context's error flag, waits (with a
-// fixed ~1 s bound) for the copies and MMAs it has in flight, frees its TMEM and
-// returns.  The flag is read back at the next host synchronisation of the context
-// and raised as IMPS_TIMEOUT; a set flag also makes every later pipeline wait give
-// up at once, so the rest of the failing call costs little.
+//   warp 1: TMEM allocator + single-thread tcgen05.mma issuer (M=128, N=BN, K=32)
+//   warps 2-9: epilogue, tcgen05.ld 32x32b, two warps per TMEM lane quarter, each
+//           owning BN/2 columns in chunks of 32; a thread sums its row's chunk over
+//           all diagonals in FP64 registers and writes it (adds it, for the later
+//           K groups of a tile).  When two tiles' accumulators fit in TMEM the
+//           epilogue of one tile overlaps the MMAs of the next.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -50,34 +47,40 @@ namespace imps {
 namespace {
 
 constexpr int BM = 128;          // tile rows (real rows of At)
-constexpr int BN = 64;           // tile cols (rows of Bt)
+constexpr int BN_MAX = 128;      // widest tile (rows of Bt); B planes are padded to it
 constexpr int KB = 64;           // K bytes per pipeline stage (one 64B swizzle row)
 constexpr int KPAD = 128;        // K padding of the slice planes (the slicing kernels' tile)
 constexpr int MAX_STAGES = 8;
 constexpr int MAX_BUF = 4;       // tile accumulator buffers in TMEM
 constexpr int EPI_WARPS = 8;     // two warps per TMEM lane quarter, each owning BN/2 columns
 constexpr int A_TILE = BM * KB;  // 8 KB per slice
-constexpr int B_TILE = BN * KB;  // 4 KB per slice
 constexpr int STAGE_BUDGET = 200 * 1024;
 constexpr int BAR_BYTES = 512;
 constexpr int NTHREADS = 32 * (2 + EPI_WARPS);
 constexpr long long DRAIN_CYCLES = 2000000000LL;  // ~1 s at 1.9 GHz: bound of the error-path drains
 
-__host__ __device__ constexpr int stages_for(int s) {
-  return (STAGE_BUDGET / (s * (A_TILE + B_TILE))) < MAX_STAGES ? (STAGE_BUDGET / (s * (A_TILE + B_TILE)))
-                                                               : MAX_STAGES;
+// tile width for a slice count: all s diagonals of a 128-column tile fit TMEM up to s = 4
+__host__ __device__ constexpr int bn_for(int s) { return (s >= 1 && s <= 4) ? 128 : 64; }
+__host__ __device__ constexpr int stages_for(int s, int bn) {
+  return (STAGE_BUDGET / (s * (A_TILE + bn * KB))) < MAX_STAGES ? (STAGE_BUDGET / (s * (A_TILE + bn * KB)))
+                                                                 : MAX_STAGES;
 }
-__host__ __device__ constexpr int bufs_for(int s) {
-  return (512 / (s * BN)) < MAX_BUF ? (512 / (s * BN)) : MAX_BUF;
+__host__ __device__ constexpr int bufs_for(int s, int bn) {
+  return (512 / (s * bn)) < MAX_BUF ? (512 / (s * bn)) : MAX_BUF;
 }
-__host__ constexpr int smem_bytes_for(int s) { return stages_for(s) * s * (A_TILE + B_TILE) + 1024 + BAR_BYTES; }
+__host__ constexpr int smem_bytes_for(int s, int bn) {
+  return stages_for(s, bn) * s * (A_TILE + bn * KB) + 1024 + BAR_BYTES;
+}
 __host__ constexpr int max_smem_bytes() {
   int m = 0;
-  for (int s = 1; s <= 8; ++s) m = smem_bytes_for(s) > m ? smem_bytes_for(s) : m;
+  for (int s = 1; s <= 8; ++s) m = smem_bytes_for(s, bn_for(s)) > m ? smem_bytes_for(s, bn_for(s)) : m;
+  for (int s = 1; s <= 8; ++s) m = smem_bytes_for(s, 64) > m ? smem_bytes_for(s, 64) : m;
   return m;
 }
 static_assert(max_smem_bytes() <= 227 * 1024, "pipeline does not fit in shared memory");
-static_assert(stages_for(8) >= 2, "at least double buffering at 8 slices");
+static_assert(bufs_for(4, 128) >= 1 && bufs_for(8, 64) >= 1, "every diagonal of a tile fits in TMEM");
+static_assert(stages_for(4, 128) >= 2, "at least double buffering at 4 slices, 128 columns");
+static_assert(stages_for(8, 64) >= 2, "at least double buffering at 8 slices");
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -147,7 +150,8 @@ __device__ __forceinline__ uint64_t make_desc(uint32_t saddr) {
   return d;
 }
 
-// instruction descriptor: kind::i8, s8 x s8 -> s32, both K-major, M = 128, N = 64
+// instruction descriptor: kind::i8, s8 x s8 -> s32, both K-major, M = 128, N = BN
+template <int BN>
 __host__ __device__ constexpr uint32_t make_idesc() {
   return (2u << 4)                 // D format: s32
          | (1u << 7)               // A format: s8
@@ -220,8 +224,9 @@ __device__ __forceinline__ void tile_coords(const GemmArgs& g, int t, int& mb, i
 // two K=32 MMAs into the diagonal's accumulator.  With a compile-time slice count the
 // loops unroll into a straight run of MMAs on precomputed descriptors, so one thread
 // keeps up with the tensor pipe.
-template <int SC>
+template <int SC, int BN>
 __device__ __forceinline__ void issue_stage(int S, uint64_t da, uint64_t db, uint32_t dt0, uint32_t idesc, bool fresh) {
+  constexpr int B_TILE = BN * KB;
   const int s = SC > 0 ? SC : S;
 #pragma unroll
   for (int d = 0; d < (SC > 0 ? SC : 8); ++d) {
@@ -241,9 +246,11 @@ __device__ __forceinline__ void issue_stage(int S, uint64_t da, uint64_t db, uin
   }
 }
 
-template <int SC>
+template <int SC, int BN>
 __global__ void __launch_bounds__(NTHREADS, 1)
     k_gemm_i8(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, const GemmArgs g) {
+  constexpr int B_TILE = BN * KB;
+  static_assert(BN % 64 == 0 && BN <= BN_MAX, "epilogue chunks of 32 columns per half tile");
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const int S = SC > 0 ? SC : g.s, NST = g.nst, NBUF = g.nbuf;
@@ -313,7 +320,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     }
   } else if (warp == 1) {
     if (lane == 0) {
-      const uint32_t idesc = make_idesc();
+      const uint32_t idesc = make_idesc<BN>();
       int stage = 0;
       uint32_t phase = 0;
       int grp = 0;  // accumulation-group counter (selects the TMEM buffer)
@@ -331,7 +338,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             tc_fence_after();
             const uint32_t a0 = smem_u32(smem + stage * stage_bytes);
             const uint32_t b0 = a0 + S * A_TILE;
-            issue_stage<SC>(S, make_desc(a0), make_desc(b0), tmem_base + (uint32_t)(buf * S * BN), idesc,
+            issue_stage<SC, BN>(S, make_desc(a0), make_desc(b0), tmem_base + (uint32_t)(buf * S * BN), idesc,
                             kb == gi.kb0);
             umma_commit(&empty[stage]);  // frees the smem stage when these MMAs retire
             if (++stage == NST) { stage = 0; phase ^= 1; }
@@ -348,48 +355,102 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     }
   } else {
     // epilogue warps 2..9: TMEM lane quarter q = warp % 4, column half h
-    constexpr int HC = BN / 2;  // columns per epilogue thread
+    constexpr int HC = BN / 2;   // columns per epilogue thread
+    constexpr int NCH = HC / 32; // chunks of 32 columns (one tcgen05.ld each per diagonal)
     const int q = warp & 3;
     const int h = (warp - 2) / 4;
     const int row = q * 32 + lane;  // tile row == TMEM lane
     double* Cd = reinterpret_cast<double*>(g.C);
-    int grp = 0;
-    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-      int mb, nb;
-      tile_coords(g, t, mb, nb);
-      // FP64 sums of this thread's row over all slice diagonals and K groups of the tile
-      double part[HC];
+    if constexpr (NCH == 1) {
+      // one chunk per thread: the row's FP64 sums are kept over all K groups of the
+      // tile and written once
+      int grp = 0;
+      for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        int mb, nb;
+        tile_coords(g, t, mb, nb);
+        double part[32];
 #pragma unroll
-      for (int j = 0; j < HC; ++j) part[j] = 0.0;
-      bool ok = true;
-      for (GroupIter gi(&g); gi.valid(); gi.next(), ++grp) {
-        const int buf = grp % NBUF;
-        if (!mbar_wait(&tfull[buf], (grp / NBUF) & 1, err, g.wait_cycles)) { ok = false; break; }
-        tc_fence_after();
-        for (int d = 0; d < S; ++d) {
-          const double w = ldexp(1.0, -7 * (d + 2));
-          int32_t r[32];
-          tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)((buf * S + d) * BN + h * HC), r);
+        for (int j = 0; j < 32; ++j) part[j] = 0.0;
+        bool ok = true;
+        for (GroupIter gi(&g); gi.valid(); gi.next(), ++grp) {
+          const int buf = grp % NBUF;
+          if (!mbar_wait(&tfull[buf], (grp / NBUF) & 1, err, g.wait_cycles)) { ok = false; break; }
+          tc_fence_after();
+          for (int d = 0; d < S; ++d) {
+            const double w = ldexp(1.0, -7 * (d + 2));
+            int32_t r[32];
+            tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)((buf * S + d) * BN + h * HC), r);
 #pragma unroll
-          for (int j = 0; j < 32; ++j) part[j] = fma((double)r[j], w, part[j]);
-        }
-        tc_fence_before();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&tempty[buf]);
-      }
-      if (!ok) break;
-      const int rr = mb * BM + row;           // real row of At
-      const int ci = rr >> 1, part_im = rr & 1;  // complex row, re/im
-      if (ci < g.Mc) {
-        const double rs = g.row_scale[ci] * g.alpha;
-#pragma unroll
-        for (int j = 0; j < HC; ++j) {
-          const int cj = nb * BN + h * HC + j;
-          if (cj < g.Nc) {
-            const double v = part[j] * rs * __ldg(&g.col_scale[cj]);
-            double* p = Cd + 2 * ((int64_t)ci + g.ldc * cj) + part_im;
-            *p = g.accumulate ? (*p + v) : v;
+            for (int j = 0; j < 32; ++j) part[j] = fma((double)r[j], w, part[j]);
           }
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&tempty[buf]);
+        }
+        if (!ok) break;
+        const int rr = mb * BM + row;              // real row of At
+        const int ci = rr >> 1, part_im = rr & 1;  // complex row, re/im
+        if (ci < g.Mc) {
+          const double rs = g.row_scale[ci] * g.alpha;
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            const int cj = nb * BN + h * HC + j;
+            if (cj < g.Nc) {
+              const double v = part[j] * rs * __ldg(&g.col_scale[cj]);
+              double* p = Cd + 2 * ((int64_t)ci + g.ldc * cj) + part_im;
+              *p = g.accumulate ? (*p + v) : v;
+            }
+          }
+        }
+      }
+    } else {
+      int grp = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+        int mb, nb;
+        tile_coords(g, t, mb, nb);
+        const int rr = mb * BM + row;              // real row of At
+        const int ci = rr >> 1, part_im = rr & 1;  // complex row, re/im
+        const double rs = (ci < g.Mc) ? g.row_scale[ci] * g.alpha : 0.0;
+        bool first = true;  // first K group of the tile writes (or adds, when accumulating)
+        for (GroupIter gi(&g); gi.valid(); gi.next(), ++grp) {
+          const int buf = grp % NBUF;
+          if (!mbar_wait(&tfull[buf], (grp / NBUF) & 1, err, g.wait_cycles)) { ok = false; break; }
+          tc_fence_after();
+#pragma unroll 1
+          for (int ch = 0; ch < NCH; ++ch) {
+            // FP64 sum of this thread's 32 columns over all slice diagonals of the group
+            double part[32];
+#pragma unroll
+            for (int j = 0; j < 32; ++j) part[j] = 0.0;
+#pragma unroll 1
+            for (int d = 0; d < S; ++d) {
+              const double w = ldexp(1.0, -7 * (d + 2));
+              int32_t r[32];
+              tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)((buf * S + d) * BN + h * HC + ch * 32), r);
+#pragma unroll
+              for (int j = 0; j < 32; ++j) part[j] = fma((double)r[j], w, part[j]);
+            }
+            if (ch == NCH - 1) {
+              // every column of this buffer has been read: hand it back to the MMA thread
+              tc_fence_before();
+              __syncwarp();
+              if (lane == 0) mbar_arrive(&tempty[buf]);
+            }
+            if (ci < g.Mc) {
+              const bool add = g.accumulate || !first;
+#pragma unroll
+              for (int j = 0; j < 32; ++j) {
+                const int cj = nb * BN + h * HC + ch * 32 + j;
+                if (cj < g.Nc) {
+                  const double v = part[j] * rs * __ldg(&g.col_scale[cj]);
+                  double* p = Cd + 2 * ((int64_t)ci + g.ldc * cj) + part_im;
+                  *p = add ? (*p + v) : v;
+                }
+              }
+            }
+          }
+          first = false;
         }
       }
     }
@@ -657,7 +718,7 @@ void split_operand_b(Context* ctx, SplitOperand& S, Op op, int K, int N, const d
   S.rows = N;
   S.K = K;
   S.s = s;
-  S.Rp = round_up(N, BN);
+  S.Rp = round_up(N, BN_MAX);  // every B box (64 or 128 rows) lies inside the planes
   S.Kp = round_up(2 * (int64_t)K, KPAD);
   const size_t plane = (size_t)S.Rp * S.Kp;
   S.data.ensure(plane * s);
@@ -692,21 +753,24 @@ void split_gemm(Context* ctx, const SplitOperand& A, const SplitOperand& B, int 
   static std::atomic<uint64_t> attr_devices{0};
   const uint64_t bit = 1ull << (ctx->device & 63);
   if (!(attr_devices.load() & bit)) {
-    for (auto k : {k_gemm_i8<0>, k_gemm_i8<2>, k_gemm_i8<3>, k_gemm_i8<4>, k_gemm_i8<5>, k_gemm_i8<6>})
+    for (auto k : {k_gemm_i8<0, 64>, k_gemm_i8<5, 64>, k_gemm_i8<6, 64>, k_gemm_i8<2, 128>, k_gemm_i8<3, 128>,
+                   k_gemm_i8<4, 128>})
       IMPS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem_bytes()));
     attr_devices.fetch_or(bit);
   }
+  // slice counts 2..4 run 128-column tiles, the rest 64-column tiles (TMEM holds s x BN columns)
+  const int bn = (s >= 2 && s <= 4) ? bn_for(s) : 64;
   const CUtensorMap mapA = make_map(static_cast<const int8_t*>(A.data.ptr), A.Kp, A.Rp, A.s, BM);
-  const CUtensorMap mapB = make_map(static_cast<const int8_t*>(B.data.ptr), B.Kp, B.Rp, B.s, BN);
+  const CUtensorMap mapB = make_map(static_cast<const int8_t*>(B.data.ptr), B.Kp, B.Rp, B.s, bn);
   GemmArgs g;
   g.num_m = (int)(A.Rp / BM);
-  g.num_n = (int)(B.Rp / BN);
+  g.num_n = (B.rows + bn - 1) / bn;  // B.Rp is a multiple of 128 >= num_n * bn
   // stream the larger operand once: consecutive CTAs share its tile and walk the other
   g.n_fast = (A.Rp * A.s >= B.Rp * B.s) ? 1 : 0;
   g.kblocks = (int)(A.Kp / KB);
   g.s = s;
-  g.nst = stages_for(s);
-  g.nbuf = bufs_for(s);
+  g.nst = stages_for(s, bn);
+  g.nbuf = bufs_for(s, bn);
   g.C = C;
   g.ldc = ldc;
   g.Mc = A.rows;
@@ -719,16 +783,17 @@ void split_gemm(Context* ctx, const SplitOperand& A, const SplitOperand& B, int 
   g.wait_cycles = ctx->wait_cycles;
   const int ntiles = g.num_m * g.num_n;
   const int grid = std::max(1, std::min(ntiles, ctx->num_sms));
+  const int smem = smem_bytes_for(s, bn);
   {
     ScopedTimer tm(ctx, "gemm_split",
-                   2.0 * (double)A.Rp * (double)B.Rp * (double)A.Kp * (double)(s * (s + 1) / 2));
+                   2.0 * (double)A.Rp * (double)g.num_n * bn * (double)A.Kp * (double)(s * (s + 1) / 2));
     switch (s) {
-      case 2: k_gemm_i8<2><<<grid, NTHREADS, smem_bytes_for(s), ctx->stream>>>(mapA, mapB, g); break;
-      case 3: k_gemm_i8<3><<<grid, NTHREADS, smem_bytes_for(s), ctx->stream>>>(mapA, mapB, g); break;
-      case 4: k_gemm_i8<4><<<grid, NTHREADS, smem_bytes_for(s), ctx->stream>>>(mapA, mapB, g); break;
-      case 5: k_gemm_i8<5><<<grid, NTHREADS, smem_bytes_for(s), ctx->stream>>>(mapA, mapB, g); break;
-      case 6: k_gemm_i8<6><<<grid, NTHREADS, smem_bytes_for(s), ctx->stream>>>(mapA, mapB, g); break;
-      default: k_gemm_i8<0><<<grid, NTHREADS, smem_bytes_for(s), ctx->stream>>>(mapA, mapB, g); break;
+      case 2: k_gemm_i8<2, 128><<<grid, NTHREADS, smem, ctx->stream>>>(mapA, mapB, g); break;
+      case 3: k_gemm_i8<3, 128><<<grid, NTHREADS, smem, ctx->stream>>>(mapA, mapB, g); break;
+      case 4: k_gemm_i8<4, 128><<<grid, NTHREADS, smem, ctx->stream>>>(mapA, mapB, g); break;
+      case 5: k_gemm_i8<5, 64><<<grid, NTHREADS, smem, ctx->stream>>>(mapA, mapB, g); break;
+      case 6: k_gemm_i8<6, 64><<<grid, NTHREADS, smem, ctx->stream>>>(mapA, mapB, g); break;
+      default: k_gemm_i8<0, 64><<<grid, NTHREADS, smem, ctx->stream>>>(mapA, mapB, g); break;
     }
     ctx->n_kernels++;
     ctx->n_gemm++;
@@ -736,7 +801,7 @@ void split_gemm(Context* ctx, const SplitOperand& A, const SplitOperand& B, int 
   }
   ctx->split_launches++;
   ctx->split_alg_flops += 8.0 * (double)A.rows * (double)B.rows * (double)A.K;
-  ctx->split_exec_ops += 2.0 * (double)A.Rp * (double)B.Rp * (double)A.Kp * (double)(s * (s + 1) / 2);
+  ctx->split_exec_ops += 2.0 * (double)A.Rp * (double)g.num_n * bn * (double)A.Kp * (double)(s * (s + 1) / 2);
   // the error flag is read at the context's next host synchronisation
   ctx->err_armed = true;
 }

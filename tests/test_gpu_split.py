@@ -84,6 +84,29 @@ def test_split_gemm_bit_exact_slice_counts(s, M, N, K):
         c.close()
 
 
+@pytest.mark.parametrize("s", [2, 3, 4])
+@pytest.mark.parametrize("M,N,K,opB", [(300, 200, 600, "N"), (520, 136, 700, "C"), (64, 200, 17000, "N")])
+def test_split_gemm_bit_exact_wide_tiles(s, M, N, K, opB):
+    # slice counts 2..4 run 128-column tiles: N ragged against 128 (the last tile part
+    # valid), and at 4 slices K = 17000 is cut into two int32-safe groups, whose later
+    # group the epilogue adds onto the first one's output
+    c = imps.Context(0)
+    try:
+        c.set_precision(L.IMPS_PREC_SPLIT_I8, s)
+        rng = np.random.default_rng(s * 7 + N + K)
+        A = rng.integers(-100, 101, (M, K)) + 1j * rng.integers(-100, 101, (M, K))
+        B0 = rng.integers(-100, 101, (K, N)) + 1j * rng.integers(-100, 101, (K, N))
+        B = B0 if opB == "N" else B0.conj().T
+        got, ref = run_gemm(c, "N", opB, A, B)
+        assert np.array_equal(got, ref), f"max diff {np.abs(got - ref).max()}"
+        # accumulate onto an existing C through the same tiles
+        C0 = rng.integers(-9, 10, (M, N)).astype(complex)
+        got2, _ = run_gemm(c, "N", opB, A, B, Cinit=C0, beta=1.0)
+        assert np.array_equal(got2, ref + C0)
+    finally:
+        c.close()
+
+
 def test_split_gemm_accumulate(split_ctx):
     rng = np.random.default_rng(7)
     A = rng.integers(-50, 51, (200, 600)) + 1j * rng.integers(-50, 51, (200, 600))
