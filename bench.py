@@ -185,12 +185,13 @@ def fp64_reference_tflops():
 
 
 # DRAM bytes per k_gemm_i8 launch: the mean of the two launches of one AC Heff apply at
-# Hubbard D=1024, s=5 (GL x: 319 MB read + 382 MB written; T2 GR: 979 MB read + 59 MB
-# written), from one ncu capture (profiles/k_gemm_i8_ac_heff_hubbard_d1024_traffic.md).
-# The algorithmic bytes of the same two launches are 573 MB and 633 MB.
-GEMM_I8_TRAFFIC_PER_LAUNCH = 0.5 * (318806528 + 381801472 + 978851840 + 58522112)
+# Hubbard D=1024, 4 slices, 128 x 128 tiles (GL x: 189 MB read + 369 MB written; T2 GR:
+# 616 MB read + 62 MB written), from one ncu capture
+# (profiles/k_gemm_i8_ac_heff_hubbard_d1024_traffic.md).  The algorithmic bytes of the same
+# two launches are 538 MB and 520 MB.
+GEMM_I8_TRAFFIC_PER_LAUNCH = 0.5 * (188907008 + 368586240 + 616073728 + 61922048)
 GEMM_I8_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum, mean of the 2 k_gemm_i8 launches of "
-                          "one AC Heff apply (Hubbard D=1024, s=5; bench.py --mode heff --D 1024); the timed "
+                          "one AC Heff apply (Hubbard D=1024, 4 slices; bench.py --mode heff --nslices 4); the timed "
                           "region mixes these with the smaller C-Heff and push launches")
 
 

@@ -23,11 +23,11 @@
 // Tile width: an M=128 MMA reads its A tile (4 KB per K=32) and B tile (BN x 32 B)
 // from shared memory, whose 128 B/clk per SM feed the int8 pipe's ~7.7k MAC/clk only
 // when BN >= ~115.  BN = 128 is used for s <= 4 (s x 128 TMEM columns still fit the
-// 512 of an SM); BN = 64 for more slices, where the MMA waits on shared memory.
+// 512 of an SM), 96 for s = 5 and 80 for s = 6 (480 columns), 64 beyond.
 //   warp 0: TMA producer (cp.async.bulk.tensor, 64B swizzle, 2-8 stages by s)
 //   warp 1: TMEM allocator + single-thread tcgen05.mma issuer (M=128, N=BN, K=32)
 //   warps 2-9: epilogue, tcgen05.ld 32x32b, two warps per TMEM lane quarter, each
-//           owning BN/2 columns in chunks of 32; a thread sums its row's chunk over
+//           owning BN/2 columns in chunks of 32, 16 or 8; a thread sums its row's chunk over
 //           all diagonals in FP64 registers and writes it (adds it, for the later
 //           K groups of a tile).  When two tiles' accumulators fit in TMEM the
 //           epilogue of one tile overlaps the MMAs of the next.
@@ -54,13 +54,16 @@ constexpr int MAX_STAGES = 8;
 constexpr int MAX_BUF = 4;       // tile accumulator buffers in TMEM
 constexpr int EPI_WARPS = 8;     // two warps per TMEM lane quarter, each owning BN/2 columns
 constexpr int A_TILE = BM * KB;  // 8 KB per slice
-constexpr int STAGE_BUDGET = 200 * 1024;
+constexpr int STAGE_BUDGET = 216 * 1024;
 constexpr int BAR_BYTES = 512;
 constexpr int NTHREADS = 32 * (2 + EPI_WARPS);
 constexpr long long DRAIN_CYCLES = 2000000000LL;  // ~1 s at 1.9 GHz: bound of the error-path drains
 
-// tile width for a slice count: all s diagonals of a 128-column tile fit TMEM up to s = 4
-__host__ __device__ constexpr int bn_for(int s) { return (s >= 1 && s <= 4) ? 128 : 64; }
+// tile width for a slice count: the widest multiple of 16 (at most 128) whose s
+// diagonals fit the 512 TMEM columns of an SM
+__host__ __device__ constexpr int bn_for(int s) {
+  return (s >= 1 && s <= 4) ? 128 : (s == 5 ? 96 : (s == 6 ? 80 : 64));
+}
 __host__ __device__ constexpr int stages_for(int s, int bn) {
   return (STAGE_BUDGET / (s * (A_TILE + bn * KB))) < MAX_STAGES ? (STAGE_BUDGET / (s * (A_TILE + bn * KB)))
                                                                  : MAX_STAGES;
@@ -185,6 +188,29 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, int32_t* r) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, int32_t* r) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, "
+      "[%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, int32_t* r) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+// CW columns of this warp's 32 TMEM lanes, one register per column
+template <int CW>
+__device__ __forceinline__ void tmem_ld(uint32_t taddr, int32_t* r) {
+  if constexpr (CW == 32) tmem_ld32(taddr, r);
+  else if constexpr (CW == 16) tmem_ld16(taddr, r);
+  else tmem_ld8(taddr, r);
+}
+
 struct GemmArgs {
   int num_m, num_n;          // tiles
   int n_fast;                // raster: 1 -> consecutive tiles walk N (A is the larger operand)
@@ -250,7 +276,7 @@ template <int SC, int BN>
 __global__ void __launch_bounds__(NTHREADS, 1)
     k_gemm_i8(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, const GemmArgs g) {
   constexpr int B_TILE = BN * KB;
-  static_assert(BN % 64 == 0 && BN <= BN_MAX, "epilogue chunks of 32 columns per half tile");
+  static_assert(BN % 16 == 0 && BN >= 64 && BN <= BN_MAX, "MMA N is a multiple of 16; half tiles of >= 32 columns");
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const int S = SC > 0 ? SC : g.s, NST = g.nst, NBUF = g.nbuf;
@@ -356,7 +382,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   } else {
     // epilogue warps 2..9: TMEM lane quarter q = warp % 4, column half h
     constexpr int HC = BN / 2;   // columns per epilogue thread
-    constexpr int NCH = HC / 32; // chunks of 32 columns (one tcgen05.ld each per diagonal)
+    constexpr int CW = (HC % 32 == 0) ? 32 : ((HC % 16 == 0) ? 16 : 8);  // columns per tcgen05.ld
+    constexpr int NCH = HC / CW; // chunks (one tcgen05.ld each per diagonal)
+    static_assert(HC % CW == 0, "half tile is a whole number of chunks");
     const int q = warp & 3;
     const int h = (warp - 2) / 4;
     const int row = q * 32 + lane;  // tile row == TMEM lane
@@ -419,17 +447,17 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           tc_fence_after();
 #pragma unroll 1
           for (int ch = 0; ch < NCH; ++ch) {
-            // FP64 sum of this thread's 32 columns over all slice diagonals of the group
-            double part[32];
+            // FP64 sum of this thread's CW columns over all slice diagonals of the group
+            double part[CW];
 #pragma unroll
-            for (int j = 0; j < 32; ++j) part[j] = 0.0;
+            for (int j = 0; j < CW; ++j) part[j] = 0.0;
 #pragma unroll 1
             for (int d = 0; d < S; ++d) {
               const double w = ldexp(1.0, -7 * (d + 2));
-              int32_t r[32];
-              tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)((buf * S + d) * BN + h * HC + ch * 32), r);
+              int32_t r[CW];
+              tmem_ld<CW>(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)((buf * S + d) * BN + h * HC + ch * CW), r);
 #pragma unroll
-              for (int j = 0; j < 32; ++j) part[j] = fma((double)r[j], w, part[j]);
+              for (int j = 0; j < CW; ++j) part[j] = fma((double)r[j], w, part[j]);
             }
             if (ch == NCH - 1) {
               // every column of this buffer has been read: hand it back to the MMA thread
@@ -440,8 +468,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             if (ci < g.Mc) {
               const bool add = g.accumulate || !first;
 #pragma unroll
-              for (int j = 0; j < 32; ++j) {
-                const int cj = nb * BN + h * HC + ch * 32 + j;
+              for (int j = 0; j < CW; ++j) {
+                const int cj = nb * BN + h * HC + ch * CW + j;
                 if (cj < g.Nc) {
                   const double v = part[j] * rs * __ldg(&g.col_scale[cj]);
                   double* p = Cd + 2 * ((int64_t)ci + g.ldc * cj) + part_im;
@@ -753,18 +781,20 @@ void split_gemm(Context* ctx, const SplitOperand& A, const SplitOperand& B, int 
   static std::atomic<uint64_t> attr_devices{0};
   const uint64_t bit = 1ull << (ctx->device & 63);
   if (!(attr_devices.load() & bit)) {
-    for (auto k : {k_gemm_i8<0, 64>, k_gemm_i8<5, 64>, k_gemm_i8<6, 64>, k_gemm_i8<2, 128>, k_gemm_i8<3, 128>,
+    for (auto k : {k_gemm_i8<0, 64>, k_gemm_i8<5, 96>, k_gemm_i8<6, 80>, k_gemm_i8<2, 128>, k_gemm_i8<3, 128>,
                    k_gemm_i8<4, 128>})
       IMPS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem_bytes()));
     attr_devices.fetch_or(bit);
   }
-  // slice counts 2..4 run 128-column tiles, the rest 64-column tiles (TMEM holds s x BN columns)
-  const int bn = (s >= 2 && s <= 4) ? bn_for(s) : 64;
+  // tile width by slice count (TMEM holds s x BN columns): 128 for 2..4 slices, 96 for 5,
+  // 80 for 6, 64 otherwise.  The B planes are padded to 128 rows; a 96- or 80-row box
+  // that reaches past them reads TMA's zero fill (and still delivers its full byte count).
+  const int bn = (s >= 2 && s <= 6) ? bn_for(s) : 64;
   const CUtensorMap mapA = make_map(static_cast<const int8_t*>(A.data.ptr), A.Kp, A.Rp, A.s, BM);
   const CUtensorMap mapB = make_map(static_cast<const int8_t*>(B.data.ptr), B.Kp, B.Rp, B.s, bn);
   GemmArgs g;
   g.num_m = (int)(A.Rp / BM);
-  g.num_n = (B.rows + bn - 1) / bn;  // B.Rp is a multiple of 128 >= num_n * bn
+  g.num_n = (B.rows + bn - 1) / bn;
   // stream the larger operand once: consecutive CTAs share its tile and walk the other
   g.n_fast = (A.Rp * A.s >= B.Rp * B.s) ? 1 : 0;
   g.kblocks = (int)(A.Kp / KB);
@@ -791,8 +821,8 @@ void split_gemm(Context* ctx, const SplitOperand& A, const SplitOperand& B, int 
       case 2: k_gemm_i8<2, 128><<<grid, NTHREADS, smem, ctx->stream>>>(mapA, mapB, g); break;
       case 3: k_gemm_i8<3, 128><<<grid, NTHREADS, smem, ctx->stream>>>(mapA, mapB, g); break;
       case 4: k_gemm_i8<4, 128><<<grid, NTHREADS, smem, ctx->stream>>>(mapA, mapB, g); break;
-      case 5: k_gemm_i8<5, 64><<<grid, NTHREADS, smem, ctx->stream>>>(mapA, mapB, g); break;
-      case 6: k_gemm_i8<6, 64><<<grid, NTHREADS, smem, ctx->stream>>>(mapA, mapB, g); break;
+      case 5: k_gemm_i8<5, 96><<<grid, NTHREADS, smem, ctx->stream>>>(mapA, mapB, g); break;
+      case 6: k_gemm_i8<6, 80><<<grid, NTHREADS, smem, ctx->stream>>>(mapA, mapB, g); break;
       default: k_gemm_i8<0, 64><<<grid, NTHREADS, smem, ctx->stream>>>(mapA, mapB, g); break;
     }
     ctx->n_kernels++;

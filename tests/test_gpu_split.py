@@ -84,12 +84,14 @@ def test_split_gemm_bit_exact_slice_counts(s, M, N, K):
         c.close()
 
 
-@pytest.mark.parametrize("s", [2, 3, 4])
+@pytest.mark.parametrize("s", [2, 3, 4, 5, 6])
 @pytest.mark.parametrize("M,N,K,opB", [(300, 200, 600, "N"), (520, 136, 700, "C"), (64, 200, 17000, "N")])
 def test_split_gemm_bit_exact_wide_tiles(s, M, N, K, opB):
-    # slice counts 2..4 run 128-column tiles: N ragged against 128 (the last tile part
-    # valid), and at 4 slices K = 17000 is cut into two int32-safe groups, whose later
-    # group the epilogue adds onto the first one's output
+    # slice counts 2..4 run 128-column tiles, 5 and 6 run 96- and 80-column tiles: N
+    # ragged against the tile (the last tile part valid, its B box partly past the
+    # 128-row padded planes for 96 / 80 columns), and at 4..6 slices K = 17000 is cut
+    # into two int32-safe groups, whose later group the epilogue adds onto the first
+    # one's output
     c = imps.Context(0)
     try:
         c.set_precision(L.IMPS_PREC_SPLIT_I8, s)
