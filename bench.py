@@ -524,30 +524,66 @@ def run_converge(args, world, rank, local):
     seed = args.seed if args.seed is not None else {"tfim": 1, "xxz": 2, "hubbard": 3}[args.model]
     As = imps.random_site_tensors([d] * N, args.D, seed)
     out = {}
+    traces = {}
     for prec in ("fp64", "split"):
         ctx = imps.Context(local)
         if prec == "split":
             ctx.set_precision(L.IMPS_PREC_SPLIT_I8, args.nslices)
         psi0 = imps.CanonicalIMPS.from_sites(As, ctx=ctx)
+        trace = []        # (iteration, seconds since the start, energy per site)
+        excl = [0.0]      # time spent evaluating the traced energies, left out of the clock
+
+        def record(it, psi, H_, envs, trace=trace, excl=excl):
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            e_it = imps.expectationvalue(psi, H_, envs).real / N
+            torch.cuda.synchronize()
+            trace.append((it, t - t0 - excl[0], e_it))
+            excl[0] += time.perf_counter() - t
+            return psi, envs
+
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        psi, envs, info = imps.find_groundstate(psi0, H, imps.VUMPS(D=args.D, maxiter=args.maxiter, tol=args.tol))
+        psi, envs, info = imps.find_groundstate(psi0, H, imps.VUMPS(D=args.D, maxiter=args.maxiter, tol=args.tol,
+                                                                    finalize=record))
         e = imps.expectationvalue(psi, H, envs).real / N
         torch.cuda.synchronize()
-        dt = time.perf_counter() - t0
+        dt = time.perf_counter() - t0 - excl[0]
+        # galerkin of iteration it is losses[it] (losses[0]: the start state)
+        traces[prec] = [(it, ts, et, info.losses[it]) for it, ts, et in trace]
         out[prec] = {"iterations": info.niter, "converged": bool(info.converged), "galerkin": info.itererr,
                      "energy_per_site": e, "wall_s": dt, "s_per_iter": dt / max(info.niter, 1)}
         if rank == 0:
             # each arm as soon as it ends, so that a run cut short still reports the first
-            print(json.dumps({"arm": prec, **out[prec]}), file=sys.stderr, flush=True)
+            print(json.dumps({"arm": prec, **out[prec], "trace": traces[prec]}), file=sys.stderr, flush=True)
         ctx.close()
+
+    def time_to(tr, g):
+        return next((ts for it, ts, et, gal in tr if gal <= g), None)
+
+    thresholds = [1e-3, 1e-4, 1e-5, 1e-6, 1e-7, 1e-8]
+    reach = {f"{g:.0e}": {"fp64_s": time_to(traces["fp64"], g), "split_s": time_to(traces["split"], g)}
+             for g in thresholds}
+    for v in reach.values():
+        v["speedup"] = (v["fp64_s"] / v["split_s"]) if (v["fp64_s"] and v["split_s"]) else None
+    common = min(len(traces["fp64"]), len(traces["split"]))
+    de_iter = [abs(traces["split"][i][2] - traces["fp64"][i][2]) for i in range(common)]
     res = {"metric": f"VUMPS to convergence ({args.model}, N={N}, D={args.D}, tol={args.tol})",
            "config": {"model": args.model, "N": N, "D": args.D, "seed": seed, "tol": args.tol,
-                      "h": args.h if args.model == "tfim" else None,
+                      "maxiter": args.maxiter, "h": args.h if args.model == "tfim" else None,
                       "nslices": args.nslices or "adaptive"},
            "fp64": out["fp64"], "split": out["split"],
            "delta_e": abs(out["split"]["energy_per_site"] - out["fp64"]["energy_per_site"]),
-           "wall_speedup": out["fp64"]["wall_s"] / out["split"]["wall_s"]}
+           "wall_speedup": out["fp64"]["wall_s"] / out["split"]["wall_s"],
+           "time_to_galerkin": reach,
+           "delta_e_same_iteration": {"first": de_iter[:5], "last": de_iter[-5:], "max_last10": max(de_iter[-10:])
+                                      if de_iter else None},
+           "galerkin_trace": {"fp64": [t[3] for t in traces["fp64"]], "split": [t[3] for t in traces["split"]]},
+           "energy_trace": {"fp64": [t[2] for t in traces["fp64"]], "split": [t[2] for t in traces["split"]]},
+           "time_trace": {"fp64": [round(t[1], 3) for t in traces["fp64"]],
+                          "split": [round(t[1], 3) for t in traces["split"]]}}
+    if args.model == "hubbard":
+        res["lieb_wu_e0"] = -2.5737293679
     if args.model == "tfim":
         import math as _m
         from scipy.integrate import quad

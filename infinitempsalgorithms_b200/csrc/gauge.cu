@@ -7,6 +7,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <string>
 
 #include "krylov.h"
 
@@ -65,6 +66,17 @@ void gauge_eigsolve(Context* ctx, int64_t n, const LinOp& op, const dcplx* c0, d
   arnoldi_dominant(ctx, n, op, c0, ev, etol, 30, 300, true);
 }
 
+// Reflector storage of site i's factorisation in a gauge sweep.
+std::string sweep_slot(int i) { return "gauge_sweep" + std::to_string(i); }
+
+// A sweep only needs its L (R) factors to go on; its AR (AL) tensors are read by the
+// transfer-matrix eigensolve that starts the next iteration (from eig_miniter on) and
+// are the result when the iteration stops.  Other sweeps leave Q unformed; `it` counts
+// the sweeps done, this one included.
+bool sweep_q_needed(double eps, double tol, int it, int maxiter, int eig_miniter) {
+  return eps < tol || it > maxiter || it >= eig_miniter;
+}
+
 }  // namespace
 
 GaugeResult uniform_leftorth(Context* ctx, imps_state* st, const std::vector<const dcplx*>& A, const dcplx* C0,
@@ -90,6 +102,7 @@ GaugeResult uniform_leftorth(Context* ctx, imps_state* st, const std::vector<con
   int it = 0;
   while (true) {
     if (it >= eig_miniter) {
+      ProfTag ptag(ctx, "gauge_eig");
       double etol = eig_tol_from(eps);
       LinOp op = [&](const dcplx* v, dcplx* out) {
         DevBuf& a = ctx->buf("gauge_tm_a", (size_t)DN * DN * sizeof(dcplx));
@@ -110,20 +123,23 @@ GaugeResult uniform_leftorth(Context* ctx, imps_state* st, const std::vector<con
         }
         gauge_eigsolve(ctx, (int64_t)DN * DN, op, st->C[N - 1].z(), ev.z(), etol, cptrs);
       }
-      DevBuf& q = ctx->buf("gauge_q", (size_t)DN * DN * sizeof(dcplx));
-      qrpos(ctx, DN, DN, ev.z(), DN, q.z(), st->C[N - 1].z());
+      qrpos(ctx, DN, DN, ev.z(), DN, nullptr, st->C[N - 1].z());  // the R factor only
     }
     zcopy(ctx, (int64_t)DN * DN, st->C[N - 1].z(), Cpre.z());
     for (int i = 0; i < N; ++i) {
       const int Dl = st->Dl(i), d = st->d[i], Dr = st->Dr(i);
       const dcplx* Cprev = st->C[(i - 1 + N) % N].z();
       zgemm(ctx, OP_N, OP_N, Dl, d * Dr, Dl, 1.0, Cprev, Dl, 0, Aw[i], Dl, 0, 0.0, M.z(), Dl, 0, 1, false);
-      qrpos(ctx, Dl * d, Dr, M.z(), (int64_t)Dl * d, st->AL[i].z(), st->C[i].z());
+      qr_factor(ctx, Dl * d, Dr, M.z(), (int64_t)Dl * d, st->C[i].z(), sweep_slot(i).c_str());
     }
     double nc = dznrm2(ctx, (int64_t)DN * DN, st->C[N - 1].z());
     zscal(ctx, (int64_t)DN * DN, 1.0 / nc, st->C[N - 1].z());
     eps = diff_norm(ctx, (int64_t)DN * DN, st->C[N - 1].z(), Cpre.z());
     ++it;
+    if (sweep_q_needed(eps, tol, it, maxiter, eig_miniter)) {
+      ProfTag ptag(ctx, "gauge_q");
+      for (int i = 0; i < N; ++i) qr_form_q(ctx, st->Dl(i) * st->d[i], st->Dr(i), st->AL[i].z(), sweep_slot(i).c_str());
+    }
     if (eps < tol || it > maxiter) {
       res.niter = it;
       res.err = eps;
@@ -156,6 +172,7 @@ GaugeResult uniform_rightorth(Context* ctx, imps_state* st, const std::vector<co
   int it = 0;
   while (true) {
     if (it >= eig_miniter) {
+      ProfTag ptag(ctx, "gauge_eig");
       double etol = eig_tol_from(eps);
       LinOp op = [&](const dcplx* v, dcplx* out) {
         DevBuf& a = ctx->buf("gauge_tm_a", (size_t)DN * DN * sizeof(dcplx));
@@ -176,20 +193,23 @@ GaugeResult uniform_rightorth(Context* ctx, imps_state* st, const std::vector<co
         }
         gauge_eigsolve(ctx, (int64_t)DN * DN, op, st->C[N - 1].z(), ev.z(), etol, cptrs);
       }
-      DevBuf& q = ctx->buf("gauge_q", (size_t)DN * DN * sizeof(dcplx));
-      lqpos(ctx, DN, DN, ev.z(), DN, st->C[N - 1].z(), q.z());
+      lqpos(ctx, DN, DN, ev.z(), DN, st->C[N - 1].z(), nullptr);  // the L factor only
     }
     zcopy(ctx, (int64_t)DN * DN, st->C[N - 1].z(), Cpre.z());
     for (int i = N - 1; i >= 0; --i) {
       const int Dl = st->Dl(i), d = st->d[i], Dr = st->Dr(i);
       zgemm(ctx, OP_N, OP_N, Dl * d, Dr, Dr, 1.0, Aw[i], (int64_t)Dl * d, 0, st->C[i].z(), Dr, 0, 0.0, M.z(),
             (int64_t)Dl * d, 0, 1, false);
-      lqpos(ctx, Dl, d * Dr, M.z(), Dl, st->C[(i - 1 + N) % N].z(), st->AR[i].z());
+      lq_factor(ctx, Dl, d * Dr, M.z(), Dl, st->C[(i - 1 + N) % N].z(), sweep_slot(i).c_str());
     }
     double nc = dznrm2(ctx, (int64_t)DN * DN, st->C[N - 1].z());
     zscal(ctx, (int64_t)DN * DN, 1.0 / nc, st->C[N - 1].z());
     eps = diff_norm(ctx, (int64_t)DN * DN, st->C[N - 1].z(), Cpre.z());
     ++it;
+    if (sweep_q_needed(eps, tol, it, maxiter, eig_miniter)) {
+      ProfTag ptag(ctx, "gauge_q");
+      for (int i = 0; i < N; ++i) lq_form_q(ctx, st->Dl(i), st->d[i] * st->Dr(i), st->AR[i].z(), sweep_slot(i).c_str());
+    }
     if (eps < tol || it > maxiter) {
       res.niter = it;
       res.err = eps;

@@ -418,29 +418,35 @@ void apply_block(Context* ctx, int R, int N, int b, const dcplx* Vp, int64_t ldv
 
 }  // namespace
 
-void qrpos(Context* ctx, int m, int n, const dcplx* M, int64_t ldm, dcplx* Q, dcplx* R) {
+// Factorisation half of QRpos: A = H_1 ... H_k [R; 0].  The explicit reflectors V, the
+// compact-WY factor of every outer block and the diagonal phases stay in the slot's
+// buffers (`<slot>_v`, `<slot>_t`, `<slot>_ph`) until the next factorisation into the
+// same slot, so that Q can be formed later (qr_form_q) or not at all.  R gets the
+// positive-diagonal phase fix.
+void qr_factor(Context* ctx, int m, int n, const dcplx* M, int64_t ldm, dcplx* R, const char* slot) {
   IMPS_REQUIRE(m > 0 && n > 0, IMPS_INVALID_ARG, "qrpos: empty matrix");
   IMPS_REQUIRE(m <= 8 * QR_G, IMPS_INVALID_ARG, "qrpos: more than 32768 rows is not supported");
   ctx->n_qr++;
   const int k = std::min(m, n);
-  const double qf = 8.0 * (2.0 * m * (double)n * k - 2.0 / 3.0 * k * (double)k * k) * 2.0;
+  const double qf = 8.0 * (2.0 * m * (double)n * k - 2.0 / 3.0 * k * (double)k * k);
   ctx->qr_flops += qf;
   ScopedTimer t(ctx, "qr", qf);
+  const std::string sl(slot);
   const int nob = (k + QR_NBO - 1) / QR_NBO;
   const int wmax = std::max({n, k, QR_NBO});
   DevBuf& Ab = ctx->buf("qr_a", (size_t)m * n * sizeof(dcplx));
-  DevBuf& Vb = ctx->buf("qr_v", (size_t)m * k * sizeof(dcplx));
+  DevBuf& Vb = ctx->buf(sl + "_v", (size_t)m * k * sizeof(dcplx));
   DevBuf& Tin = ctx->buf("qr_tin", (size_t)(QR_NBO / 2) * QR_NBMAX * QR_NBMAX * sizeof(dcplx));
-  DevBuf& Tbig = ctx->buf("qr_t", (size_t)nob * QR_NBO * QR_NBO * sizeof(dcplx));
+  DevBuf& Tbig = ctx->buf(sl + "_t", (size_t)nob * QR_NBO * QR_NBO * sizeof(dcplx));
   DevBuf& Gb = ctx->buf("qr_g", (size_t)QR_NBO * QR_NBO * sizeof(dcplx));
   DevBuf& taub = ctx->buf("qr_tau", (size_t)k * sizeof(dcplx));
-  DevBuf& ph = ctx->buf("qr_ph", (size_t)k * sizeof(dcplx));
+  DevBuf& ph = ctx->buf(sl + "_ph", (size_t)k * sizeof(dcplx));
   DevBuf& Wb = ctx->buf("qr_w", (size_t)QR_NBO * wmax * sizeof(dcplx));
   DevBuf& Yb = ctx->buf("qr_y", (size_t)QR_NBO * m * sizeof(dcplx));
   DevBuf& Pb = ctx->buf("qr_part", (size_t)QR_NBO * wmax * QR_MAXCHUNK * sizeof(dcplx));
   zcopy2d(ctx, m, n, M, ldm, Ab.z(), m);
   dcplx* A = Ab.z();
-  std::vector<std::pair<int, int>> blocks;  // (P, bo)
+  int nblk = 0;
   for (int P = 0; P < k;) {
     const int bo = std::min(QR_NBO, k - P);
     PanelList pl;
@@ -473,7 +479,7 @@ void qrpos(Context* ctx, int m, int n, const dcplx* M, int64_t ldm, dcplx* Q, dc
     // compact-WY factor of the outer block, then its trailing update
     const int RrB = m - P;
     dcplx* Vblk = Vb.z() + P + (int64_t)m * P;
-    dcplx* Tb = Tbig.z() + (size_t)blocks.size() * QR_NBO * QR_NBO;
+    dcplx* Tb = Tbig.z() + (size_t)nblk * QR_NBO * QR_NBO;
     if (pl.n > 1) gemm_xhv(ctx, bo, bo, RrB, Vblk, Vblk, m, Pb.z(), Gb.z());
     static DeviceOnce merge_attr;
     merge_attr.run(ctx->device, [] {
@@ -487,7 +493,7 @@ void qrpos(Context* ctx, int m, int n, const dcplx* M, int64_t ldm, dcplx* Q, dc
       gemm_xhv(ctx, n2, bo, RrB, A2, Vblk, m, Pb.z(), Wb.z());
       apply_block(ctx, RrB, n2, bo, Vblk, m, Tb, bo, OP_C, Wb.z(), Yb.z(), A2, m);
     }
-    blocks.push_back({P, bo});
+    ++nblk;
     P += bo;
   }
   {
@@ -496,11 +502,30 @@ void qrpos(Context* ctx, int m, int n, const dcplx* M, int64_t ldm, dcplx* Q, dc
     k_extract_r<<<std::max(g, 1), 256, 0, ctx->stream>>>(k, n, A, m, R, k, ph.z());
     ctx->n_kernels++;
   }
-  // Q = H_1 ... H_k [I; 0], outer block reflectors applied from the last block back
+  scale_q_r(ctx, 0, n, k, nullptr, 1, R, k, ph.z());  // R rows by conj(phase)
+}
+
+// Q (m x k, ld m) of the last qr_factor(m, n, ...) into `slot`:
+// Q = H_1 ... H_k [I; 0] with the outer blocks applied from the last back, then the
+// columns scaled by the diagonal phases (the positive-diagonal convention of QRpos).
+void qr_form_q(Context* ctx, int m, int n, dcplx* Q, const char* slot) {
+  const int k = std::min(m, n);
+  const double qf = 8.0 * (2.0 * m * (double)n * k - 2.0 / 3.0 * k * (double)k * k);
+  ctx->qr_flops += qf;
+  ScopedTimer t(ctx, "qr", qf);
+  const std::string sl(slot);
+  const int nob = (k + QR_NBO - 1) / QR_NBO;
+  const int wmax = std::max({n, k, QR_NBO});
+  DevBuf& Vb = ctx->buf(sl + "_v", (size_t)m * k * sizeof(dcplx));
+  DevBuf& Tbig = ctx->buf(sl + "_t", (size_t)nob * QR_NBO * QR_NBO * sizeof(dcplx));
+  DevBuf& ph = ctx->buf(sl + "_ph", (size_t)k * sizeof(dcplx));
+  DevBuf& Wb = ctx->buf("qr_w", (size_t)QR_NBO * wmax * sizeof(dcplx));
+  DevBuf& Yb = ctx->buf("qr_y", (size_t)QR_NBO * m * sizeof(dcplx));
+  DevBuf& Pb = ctx->buf("qr_part", (size_t)QR_NBO * wmax * QR_MAXCHUNK * sizeof(dcplx));
   zfill2d(ctx, m, k, 0.0, Q, m);
   zadd_diag(ctx, k, Q, m, 1.0);
-  for (int t = (int)blocks.size() - 1; t >= 0; --t) {
-    const int P = blocks[t].first, bo = blocks[t].second;
+  for (int t = nob - 1; t >= 0; --t) {
+    const int P = t * QR_NBO, bo = std::min(QR_NBO, k - P);
     const int RrB = m - P, nc = k - P;
     dcplx* Vblk = Vb.z() + P + (int64_t)m * P;
     dcplx* Tb = Tbig.z() + (size_t)t * QR_NBO * QR_NBO;
@@ -508,19 +533,34 @@ void qrpos(Context* ctx, int m, int n, const dcplx* M, int64_t ldm, dcplx* Q, dc
     gemm_xhv(ctx, nc, bo, RrB, Qs, Vblk, m, Pb.z(), Wb.z());
     apply_block(ctx, RrB, nc, bo, Vblk, m, Tb, bo, OP_N, Wb.z(), Yb.z(), Qs, m);
   }
-  scale_q_r(ctx, m, n, k, Q, m, R, k, ph.z());
+  scale_q_r(ctx, m, 0, k, Q, m, nullptr, k, ph.z());  // Q columns by phase
+}
+
+void qrpos(Context* ctx, int m, int n, const dcplx* M, int64_t ldm, dcplx* Q, dcplx* R) {
+  qr_factor(ctx, m, n, M, ldm, R, "qr");
+  if (Q) qr_form_q(ctx, m, n, Q, "qr");
+}
+
+// M (m x n) = L Q  <=>  M^H = Q^H L^H : QRpos of M^H (n x m) gives Q' (n x k), R' (k x m)
+void lq_factor(Context* ctx, int m, int n, const dcplx* M, int64_t ldm, dcplx* L, const char* slot) {
+  const int k = std::min(m, n);
+  DevBuf& MH = ctx->buf("lq_mh", (size_t)m * n * sizeof(dcplx));
+  DevBuf& Rp = ctx->buf("lq_r", (size_t)k * m * sizeof(dcplx));
+  zconj_transpose(ctx, m, n, M, ldm, MH.z(), n);
+  qr_factor(ctx, n, m, MH.z(), n, Rp.z(), slot);
+  zconj_transpose(ctx, k, m, Rp.z(), k, L, m);  // L = R'^H  (m x k)
+}
+
+void lq_form_q(Context* ctx, int m, int n, dcplx* Q, const char* slot) {
+  const int k = std::min(m, n);
+  DevBuf& Qp = ctx->buf("lq_q", (size_t)n * k * sizeof(dcplx));
+  qr_form_q(ctx, n, m, Qp.z(), slot);
+  zconj_transpose(ctx, n, k, Qp.z(), n, Q, k);  // Q = Q'^H  (k x n)
 }
 
 void lqpos(Context* ctx, int m, int n, const dcplx* M, int64_t ldm, dcplx* L, dcplx* Q) {
-  // M (m x n) = L Q  <=>  M^H = Q^H L^H : QRpos of M^H (n x m) gives Q' (n x k), R' (k x m)
-  const int k = std::min(m, n);
-  DevBuf& MH = ctx->buf("lq_mh", (size_t)m * n * sizeof(dcplx));
-  DevBuf& Qp = ctx->buf("lq_q", (size_t)n * k * sizeof(dcplx));
-  DevBuf& Rp = ctx->buf("lq_r", (size_t)k * m * sizeof(dcplx));
-  zconj_transpose(ctx, m, n, M, ldm, MH.z(), n);
-  qrpos(ctx, n, m, MH.z(), n, Qp.z(), Rp.z());
-  zconj_transpose(ctx, k, m, Rp.z(), k, L, m);   // L = R'^H  (m x k)
-  zconj_transpose(ctx, n, k, Qp.z(), n, Q, k);   // Q = Q'^H  (k x n)
+  lq_factor(ctx, m, n, M, ldm, L, "qr");
+  if (Q) lq_form_q(ctx, m, n, Q, "qr");
 }
 
 }  // namespace imps

@@ -378,6 +378,13 @@ void zcopy2d(Context* ctx, int rows, int cols, const dcplx* X, int64_t ldx, dcpl
 // Q overwrites nothing: results go to Q (m x k) and R (k x n), k = min(m, n).
 void qrpos(Context* ctx, int m, int n, const dcplx* M, int64_t ldm, dcplx* Q, dcplx* R);
 void lqpos(Context* ctx, int m, int n, const dcplx* M, int64_t ldm, dcplx* L, dcplx* Q);
+// The two halves of QRpos / LQpos: the factorisation (R or L, phase-fixed) keeps its
+// reflectors in the named slot; Q is formed from them on request, any time before the
+// next factorisation into the same slot.  Q == nullptr in qrpos / lqpos skips Q.
+void qr_factor(Context* ctx, int m, int n, const dcplx* M, int64_t ldm, dcplx* R, const char* slot);
+void qr_form_q(Context* ctx, int m, int n, dcplx* Q, const char* slot);
+void lq_factor(Context* ctx, int m, int n, const dcplx* M, int64_t ldm, dcplx* L, const char* slot);
+void lq_form_q(Context* ctx, int m, int n, dcplx* Q, const char* slot);
 
 // Reads the device error flag if a kernel that may set it ran since the last check
 // (synchronises the stream); a set flag is cleared and raised as IMPS_TIMEOUT.
