@@ -556,12 +556,15 @@ __global__ void k_scales(int n, const unsigned long long* __restrict__ mx, doubl
 }
 
 __device__ __forceinline__ void slice_value(double x, int s, int8_t* out) {
-  // x in (-1, 1): out[t] = trunc(x * 128); x = x * 128 - out[t]
+  // x in (-1, 1): the s leading base-128 digits of x, truncated toward zero, each with
+  // the sign of x (x = sum_t out[t] 128^-(t+1) + r, |r| < 128^-s).  x 2^(7s) is exact
+  // (a power-of-two scaling below 2^56), so its integer part carries all s digits.
+  const double y = ldexp(x, 7 * s);
+  const long long n = (fabs(y) < 9.0e18) ? (long long)y : 0;  // non-finite input: zero slices
+  const long long a = n < 0 ? -n : n;
   for (int t = 0; t < s; ++t) {
-    double v = x * 128.0;
-    double a = trunc(v);
-    out[t] = (int8_t)a;
-    x = v - a;
+    const int dg = (int)((a >> (7 * (s - 1 - t))) & 127);
+    out[t] = (int8_t)(n < 0 ? -dg : dg);
   }
 }
 

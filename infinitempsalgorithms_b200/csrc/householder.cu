@@ -381,6 +381,159 @@ int panel_width(int R) {
   return 2;
 }
 
+// Small-product path for the updates inside an outer block (N <= 48 columns against
+// b <= 16 reflectors): on these shapes a DMMA GEMM launch is all pipeline fill, so one
+// kernel forms the long-K product and a second applies it.
+constexpr int XS_NT = 256;   // threads of the X^H V kernel
+constexpr int XS_ROWS = 64;  // rows staged in shared memory per step (one step per CTA)
+constexpr int XS_MAXO = 16;  // outputs per thread: N b <= 4096
+constexpr int XS_LD = XS_ROWS + 1;
+
+// Wh (N x b, ld N) = X^H V over K rows, X (K x N) and V (K x b) with leading dimension ld.
+// CTA g sums rows [g kc, (g + 1) kc) into part[g]; the last CTA to finish (counter) adds
+// the partials in CTA order, so the result does not depend on scheduling, resets the
+// counter and, when T is given, forms Z (b x N, ld b) = op(T) Wh^H (op = C or N).
+__global__ void __launch_bounds__(XS_NT) k_xhv_small(int K, int N, int b, int kc, const dcplx* __restrict__ X,
+                                                      const dcplx* __restrict__ Vm, int64_t ld,
+                                                      dcplx* __restrict__ part, unsigned* __restrict__ counter,
+                                                      dcplx* __restrict__ Wh, const dcplx* __restrict__ T, int ldt,
+                                                      int conjT, dcplx* __restrict__ Z) {
+  extern __shared__ dcplx sh[];  // [N + b columns][XS_LD rows], later the summed Wh
+  __shared__ bool last;
+  const int nb = N * b, W = N + b, tid = threadIdx.x;
+  const int k0 = blockIdx.x * kc, k1 = min(K, k0 + kc);
+  dcplx acc[XS_MAXO];
+#pragma unroll
+  for (int i = 0; i < XS_MAXO; ++i) acc[i] = make_double2(0.0, 0.0);
+  for (int r0 = k0; r0 < k1; r0 += XS_ROWS) {
+    const int nr = min(XS_ROWS, k1 - r0);
+    __syncthreads();
+    for (int e = tid; e < XS_ROWS * W; e += XS_NT) {
+      const int r = e % XS_ROWS, col = e / XS_ROWS;  // consecutive threads walk rows: coalesced
+      dcplx v = make_double2(0.0, 0.0);
+      if (r < nr) v = (col < N) ? X[(int64_t)(r0 + r) + ld * col] : Vm[(int64_t)(r0 + r) + ld * (col - N)];
+      sh[r + XS_LD * col] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < XS_MAXO; ++i) {
+      const int o = tid + XS_NT * i;
+      if (o < nb) {
+        const dcplx* xc = sh + XS_LD * (o % N);
+        const dcplx* vc = sh + XS_LD * (N + o / N);
+        for (int r = 0; r < nr; ++r) {
+          const dcplx x = xc[r], v = vc[r];
+          acc[i].x = fma(x.x, v.x, fma(x.y, v.y, acc[i].x));
+          acc[i].y = fma(x.x, v.y, fma(-x.y, v.x, acc[i].y));
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < XS_MAXO; ++i) {
+    const int o = tid + XS_NT * i;
+    if (o < nb) part[(int64_t)blockIdx.x * nb + o] = acc[i];
+  }
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  __syncthreads();
+  for (int o = tid; o < nb; o += XS_NT) {
+    dcplx t = make_double2(0.0, 0.0);
+    int g = 0;
+    for (; g + 4 <= (int)gridDim.x; g += 4) {  // four loads in flight, added in CTA order
+      const dcplx v0 = __ldcg(&part[(int64_t)g * nb + o]), v1 = __ldcg(&part[(int64_t)(g + 1) * nb + o]);
+      const dcplx v2 = __ldcg(&part[(int64_t)(g + 2) * nb + o]), v3 = __ldcg(&part[(int64_t)(g + 3) * nb + o]);
+      t.x += v0.x; t.y += v0.y;
+      t.x += v1.x; t.y += v1.y;
+      t.x += v2.x; t.y += v2.y;
+      t.x += v3.x; t.y += v3.y;
+    }
+    for (; g < (int)gridDim.x; ++g) {
+      const dcplx v = __ldcg(&part[(int64_t)g * nb + o]);
+      t.x += v.x;
+      t.y += v.y;
+    }
+    Wh[o] = t;
+    sh[o] = t;  // nb <= XS_LD * (N + b)
+  }
+  if (tid == 0) *counter = 0u;
+  if (!Z) return;
+  __syncthreads();
+  // Z[i, n] = sum_l op(T)[i, l] conj(Wh[n, l])
+  for (int e = tid; e < nb; e += XS_NT) {
+    const int i = e % b, n = e / b;
+    dcplx z = make_double2(0.0, 0.0);
+    for (int l = 0; l < b; ++l) {
+      dcplx t = conjT ? T[l + (int64_t)ldt * i] : T[i + (int64_t)ldt * l];
+      if (conjT) t.y = -t.y;
+      const dcplx w = sh[n + N * l];  // conj(w) below
+      z.x += t.x * w.x + t.y * w.y;
+      z.y += t.y * w.x - t.x * w.y;
+    }
+    Z[e] = z;
+  }
+}
+
+// A2 (R x N, lda) -= V (R x b, ldv) Z (b x N), b <= 16, N <= 64: a thread per element,
+// 64 rows x 4 columns per CTA (row loads coalesced, V rows shared through L1).
+__global__ void __launch_bounds__(256) k_apply_small(int R, int N, int b, const dcplx* __restrict__ Vm, int64_t ldv,
+                                                     const dcplx* __restrict__ Z, dcplx* __restrict__ A2,
+                                                     int64_t lda) {
+  const int r = blockIdx.x * 64 + (threadIdx.x & 63);
+  const int n = blockIdx.y * 4 + (threadIdx.x >> 6);
+  if (r >= R || n >= N) return;
+  dcplx a = A2[r + lda * n];
+#pragma unroll
+  for (int i = 0; i < QR_NBMAX; ++i) {
+    if (i < b) {
+      const dcplx v = Vm[r + ldv * i], z = __ldg(&Z[i + b * n]);
+      a.x -= v.x * z.x - v.y * z.y;
+      a.y -= v.x * z.y + v.y * z.x;
+    }
+  }
+  A2[r + lda * n] = a;
+}
+
+// Wh = X^H V (and Z = op(T) Wh^H when T is given) by k_xhv_small.
+void xhv_small(Context* ctx, int N, int b, int K, const dcplx* X, const dcplx* Vm, int64_t ld, dcplx* part,
+               dcplx* Wh, const dcplx* T, int ldt, bool conjT, dcplx* Z) {
+  IMPS_REQUIRE(N * b <= XS_NT * XS_MAXO && N <= QR_NBO && b <= QR_NBO, IMPS_INVALID_ARG, "xhv_small: shape");
+  DevBuf& cnt = ctx->buf("qr_xhv_count", 256);
+  if (ctx->qr_count_ptr != cnt.ptr) {  // a new counter starts at zero; each launch leaves it at zero
+    IMPS_CUDA(cudaMemsetAsync(cnt.ptr, 0, 256, ctx->stream));
+    ctx->qr_count_ptr = cnt.ptr;
+  }
+  // one staged chunk of XS_ROWS rows per CTA, at most 64 partials (more rows per CTA past
+  // that): the last CTA sums g N b values
+  int g = std::max(1, std::min(64, (K + XS_ROWS - 1) / XS_ROWS));
+  const int kc = (K + g - 1) / g;
+  g = (K + kc - 1) / kc;
+  ScopedTimer tm(ctx, "qr_small", 8.0 * N * b * (double)K);
+  const size_t smem = (size_t)XS_LD * (N + b) * sizeof(dcplx);
+  static DeviceOnce attr;
+  attr.run(ctx->device, [] {
+    IMPS_CUDA(cudaFuncSetAttribute(k_xhv_small, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)((size_t)XS_LD * 2 * QR_NBO * sizeof(dcplx))));
+  });
+  k_xhv_small<<<g, XS_NT, smem, ctx->stream>>>(K, N, b, kc, X, Vm, ld, part, static_cast<unsigned*>(cnt.ptr), Wh,
+                                               T, ldt, conjT ? 1 : 0, Z);
+  ctx->n_kernels++;
+  IMPS_CUDA(cudaPeekAtLastError());
+}
+
+void apply_small(Context* ctx, int R, int N, int b, const dcplx* Vm, int64_t ldv, const dcplx* Z, dcplx* A2,
+                 int64_t lda) {
+  IMPS_REQUIRE(b <= QR_NBMAX && N <= QR_NBO, IMPS_INVALID_ARG, "apply_small: shape");
+  ScopedTimer tm(ctx, "qr_small", 8.0 * R * N * (double)b);
+  k_apply_small<<<dim3((R + 63) / 64, (N + 3) / 4), 256, 0, ctx->stream>>>(R, N, b, Vm, ldv, Z, A2, lda);
+  ctx->n_kernels++;
+  IMPS_CUDA(cudaPeekAtLastError());
+}
+
 // Wh (N x b, ld N) = X^H V with X (K x N) and V (K x b) sharing the leading dimension ld
 // and a long K.  The long side N goes on the GEMM's 128-row output tile; K is split into
 // row chunks (one batched GEMM over the full chunks and one for the remainder) so that
@@ -443,7 +596,10 @@ void qr_factor(Context* ctx, int m, int n, const dcplx* M, int64_t ldm, dcplx* R
   DevBuf& ph = ctx->buf(sl + "_ph", (size_t)k * sizeof(dcplx));
   DevBuf& Wb = ctx->buf("qr_w", (size_t)QR_NBO * wmax * sizeof(dcplx));
   DevBuf& Yb = ctx->buf("qr_y", (size_t)QR_NBO * m * sizeof(dcplx));
-  DevBuf& Pb = ctx->buf("qr_part", (size_t)QR_NBO * wmax * QR_MAXCHUNK * sizeof(dcplx));
+  // partial products: the split-K GEMMs' chunks, or k_xhv_small's (up to 2 CTAs per SM)
+  DevBuf& Pb = ctx->buf("qr_part", std::max((size_t)QR_NBO * wmax * QR_MAXCHUNK,
+                                            (size_t)2 * ctx->num_sms * QR_NBO * QR_NBO) * sizeof(dcplx));
+  DevBuf& Zb = ctx->buf("qr_z", (size_t)QR_NBMAX * QR_NBO * sizeof(dcplx));
   zcopy2d(ctx, m, n, M, ldm, Ab.z(), m);
   dcplx* A = Ab.z();
   int nblk = 0;
@@ -469,9 +625,10 @@ void qr_factor(Context* ctx, int m, int n, const dcplx* M, int64_t ldm, dcplx* R
       pl.n++;
       const int n2in = P + bo - (p + b);
       if (n2in > 0) {
+        // A2 <- A2 - V T^H (A2^H V)^H for the rest of the outer block
         dcplx* A2 = A + p + (int64_t)m * (p + b);
-        gemm_xhv(ctx, n2in, b, Rr, A2, Vp, m, Pb.z(), Wb.z());
-        apply_block(ctx, Rr, n2in, b, Vp, m, Tp, QR_NBMAX, OP_C, Wb.z(), Yb.z(), A2, m);
+        xhv_small(ctx, n2in, b, Rr, A2, Vp, m, Pb.z(), Wb.z(), Tp, QR_NBMAX, true, Zb.z());
+        apply_small(ctx, Rr, n2in, b, Vp, m, Zb.z(), A2, m);
       }
       p += b;
     }

@@ -113,6 +113,7 @@ struct Context {
   int* err_dev = nullptr;
   int* err_host = nullptr;
   bool err_armed = false;
+  void* qr_count_ptr = nullptr;       // completion counter of the QR small products, zeroed at this address
   long long wait_cycles = 2000000000LL;  // bound of each pipeline wait (~1 s at 1.9 GHz)
   // profiling
   bool profile = false;
