@@ -129,6 +129,13 @@ class Clocks:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            # a timed iteration that overlapped nvidia-smi's start-up ran about 0.6 s
+            # long; wait for its first sample, so the start-up is over before the timed
+            # region begins (bounded: 10 s)
+            t0 = time.time()
+            while not self.samples and self.proc.poll() is None and time.time() - t0 < 10.0:
+                time.sleep(0.02)
+            self.samples.clear()
         except Exception:
             self.proc = None
 

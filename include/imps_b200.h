@@ -103,8 +103,9 @@ int imps_ctx_destroy(imps_ctx* ctx);
 /* Use a caller-owned cudaStream_t (e.g. the host framework's current stream). */
 int imps_ctx_set_stream(imps_ctx* ctx, void* cuda_stream);
 /* Precision of the Heff/transfer contractions: IMPS_PREC_FP64 or
- * IMPS_PREC_SPLIT_I8 with `nslices` int8 slices per operand (2..7); nslices <= 0
- * selects slices per call from the requested solver tolerance. */
+ * IMPS_PREC_SPLIT_I8 with `nslices` int8 slices per operand (2..8, each slice adding
+ * 7 bits); nslices <= 0 selects slices per call from the requested solver tolerance
+ * (up to 6; a tolerance that needs more runs the FP64 engine). */
 int imps_ctx_set_precision(imps_ctx* ctx, int mode, int nslices);
 int imps_ctx_synchronize(imps_ctx* ctx);
 /* Bound of each pipeline wait inside the split GEMM kernel, in SM clock cycles

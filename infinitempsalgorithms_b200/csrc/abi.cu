@@ -179,7 +179,7 @@ int imps_ctx_set_stream(imps_ctx* h, void* stream) {
 int imps_ctx_set_precision(imps_ctx* h, int mode, int nslices) {
   if (!h) return IMPS_INVALID_ARG;
   if (mode != IMPS_PREC_FP64 && mode != IMPS_PREC_SPLIT_I8) return IMPS_INVALID_ARG;
-  if (nslices > 7) return IMPS_INVALID_ARG;
+  if (nslices > 8) return IMPS_INVALID_ARG;
   if (mode == IMPS_PREC_SPLIT_I8 && nslices > 0 && nslices < 2) return IMPS_INVALID_ARG;
   h->c.precision = mode;
   h->c.adaptive_slices = nslices <= 0;

@@ -46,9 +46,11 @@ double diff_norm(Context* ctx, int64_t n, const dcplx* a, const dcplx* b) {
 // The transfer-matrix eigensolve of a gauge sweep.  Its fixed point only seeds the next
 // sweep, whose own FP64 convergence test decides, so the products may run on the split
 // engine at a tenth of the eigensolver tolerance (the site tensors are constant over the
-// eigensolve: their splits are cached).  When that tolerance needs FP64 products, a
-// split-engine solve to 1e-8 seeds the FP64 solve, which then needs fewer FP64 products
-// for the same convergence test.
+// eigensolve: their splits are cached).  When that tolerance needs more than six slices,
+// a solve to 1e-8 at up to six slices seeds a solve whose products use up to eight
+// (truncation below 2^-56 of the row and column scales, the accuracy of an FP64 product;
+// about 1.8x faster than the FP64 engine on the 1024 x 4096 x 1024 products of d = 4,
+// D = 1024).
 void gauge_eigsolve(Context* ctx, int64_t n, const LinOp& op, const dcplx* c0, dcplx* ev, double etol,
                     const std::vector<const void*>& cptrs) {
   ConstScope cs(ctx, cptrs);
@@ -59,6 +61,8 @@ void gauge_eigsolve(Context* ctx, int64_t n, const LinOp& op, const dcplx* c0, d
       SplitAllowScope sa(ctx, 1e-9);
       arnoldi_dominant(ctx, n, op, c0, seed.z(), 1e-8, 30, 300, true);
     }
+    SplitAllowScope sa(ctx, 0.1 * etol);
+    MaxSlicesScope ms(ctx, 8);
     arnoldi_dominant(ctx, n, op, seed.z(), ev, etol, 30, 300, true);
     return;
   }

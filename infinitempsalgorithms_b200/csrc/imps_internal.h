@@ -98,6 +98,7 @@ struct Context {
   bool own_stream = true;
   int precision = PREC_FP64;
   int nslices = 5;           // int8 slices per operand in split mode
+  int max_adaptive_slices = 6;  // adaptive mode: a tolerance needing more slices runs in FP64
   bool adaptive_slices = false;
   int fp64_engine = 0;       // FP64 GEMM kernel: 0 = DMMA tensor cores, 1 = SIMT DFMA (env IMPS_FP64_ENGINE)
   std::string last_error;
@@ -135,6 +136,10 @@ struct Context {
   std::multiset<const void*> const_ptrs;
   std::map<SplitKey, std::shared_ptr<SplitOperand>> split_cache;
   std::shared_ptr<SplitOperand> split_scratch[2];
+  // split operands released by a ConstScope, kept (with their device buffers) for the
+  // next constant operands: no cudaMalloc / cudaFree, and so no implicit device
+  // synchronisation, per solve
+  std::vector<std::shared_ptr<SplitOperand>> split_pool;
   int64_t split_calls = 0, split_cache_hits = 0;
   // split GEMM launches, their algorithmic work (8 M N K real flops of the complex
   // product each computes) and the int8 operations the tensor pipe executes for it
@@ -171,8 +176,13 @@ struct ConstScope {
       if (it != ctx->const_ptrs.end()) ctx->const_ptrs.erase(it);
       if (ctx->const_ptrs.count(q) == 0) {
         for (auto it2 = ctx->split_cache.begin(); it2 != ctx->split_cache.end();) {
-          if (std::get<0>(it2->first) == q) it2 = ctx->split_cache.erase(it2);
-          else ++it2;
+          if (std::get<0>(it2->first) == q) {
+            ctx->split_pool.push_back(std::move(it2->second));
+            if (ctx->split_pool.size() > 8) ctx->split_pool.erase(ctx->split_pool.begin());
+            it2 = ctx->split_cache.erase(it2);
+          } else {
+            ++it2;
+          }
         }
       }
     }
@@ -227,6 +237,13 @@ struct SplitAllowScope {
     }
   }
 };
+// Raises the most slices the adaptive split engine may use while alive (above it: FP64).
+struct MaxSlicesScope {
+  Context* ctx;
+  int old;
+  MaxSlicesScope(Context* c, int s) : ctx(c), old(c->max_adaptive_slices) { ctx->max_adaptive_slices = s; }
+  ~MaxSlicesScope() { ctx->max_adaptive_slices = old; }
+};
 // Sets the accuracy the split GEMMs must meet while alive.
 struct TolScope {
   Context* ctx;
@@ -238,7 +255,7 @@ struct TolScope {
 // Slices the split engine would use right now (0 = FP64 engine).  Adaptive mode picks
 // the smallest s whose truncation floor meets ctx->split_tol; s >= 7 falls back to FP64.
 int active_slices(const Context* ctx);
-// the smallest slice count whose truncation floor meets tol (7 or more: the FP64 engine)
+// the smallest slice count whose truncation floor meets tol (clamped to 2..8)
 int slices_for_tol(double tol);
 // Relative accuracy of the GEMM engine currently selected (0 for FP64).
 double split_floor(const Context* ctx);

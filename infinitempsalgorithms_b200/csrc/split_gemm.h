@@ -24,7 +24,7 @@ void split_operand_b(Context* ctx, SplitOperand& S, Op op, int K, int N, const d
 void split_gemm(Context* ctx, const SplitOperand& A, const SplitOperand& B, int s, double alpha, bool accumulate,
                 dcplx* C, int64_t ldc);
 
-// Slices needed for a requested relative accuracy `tol` (clamped to 2..7).
+// Slices needed for a requested relative accuracy `tol` (clamped to 2..8).
 int slices_for_tol(double tol);
 
 }  // namespace imps

@@ -370,15 +370,17 @@ void zgemm_fp64(Context* ctx, Op opA, Op opB, int M, int N, int K, cplx alpha, c
 int slices_for_tol(double tol) {
   // the truncation error of s slices is below 2^-7s of the row/column scales; keep
   // a 2^4 margin for the sum over K and the spread inside a row
-  if (!(tol > 0)) return 7;
+  if (!(tol > 0)) return 8;
   int s = (int)std::ceil((-std::log2(tol) + 4.0) / 7.0);
-  return std::min(7, std::max(2, s));
+  return std::min(8, std::max(2, s));
 }
 
 int active_slices(const Context* ctx) {
   if (ctx->precision != PREC_SPLIT_I8 || ctx->force_fp64 > 0) return 0;
-  const int s = ctx->adaptive_slices ? slices_for_tol(ctx->split_tol) : ctx->nslices;
-  return s >= 7 ? 0 : s;  // seven slices cost about as much as the FP64 engine
+  if (!ctx->adaptive_slices) return ctx->nslices;  // a fixed count is used as given
+  // adaptive: beyond max_adaptive_slices (6 unless a scope raises it) the FP64 engine
+  const int s = slices_for_tol(ctx->split_tol);
+  return s > ctx->max_adaptive_slices ? 0 : s;
 }
 
 double split_floor(const Context* ctx) {
@@ -399,7 +401,23 @@ static std::shared_ptr<SplitOperand> get_split(Context* ctx, int side, Op op, in
   }
   std::shared_ptr<SplitOperand> S;
   if (constant) {
-    S = std::make_shared<SplitOperand>();
+    // reuse a pooled operand: the smallest whose planes already fit, else the largest
+    auto rup = [](int64_t x) { return (x + 127) / 128 * 128; };
+    const size_t need = (size_t)(side == 0 ? rup(2 * (int64_t)rows) : rup(rows)) * rup(2 * (int64_t)K) * s;
+    int best = -1;
+    for (int i = 0; i < (int)ctx->split_pool.size(); ++i) {
+      const size_t have = ctx->split_pool[i]->data.bytes;
+      if (best < 0) { best = i; continue; }
+      const size_t cur = ctx->split_pool[best]->data.bytes;
+      const bool fits = have >= need, cur_fits = cur >= need;
+      if ((fits && (!cur_fits || have < cur)) || (!fits && !cur_fits && have > cur)) best = i;
+    }
+    if (best >= 0) {
+      S = ctx->split_pool[best];
+      ctx->split_pool.erase(ctx->split_pool.begin() + best);
+    } else {
+      S = std::make_shared<SplitOperand>();
+    }
   } else {
     // transient operand: reuse one scratch object per side of this context
     if (!ctx->split_scratch[side]) ctx->split_scratch[side] = std::make_shared<SplitOperand>();
